@@ -1,0 +1,487 @@
+#!/usr/bin/env python
+"""Benchmark of the four-phonon scattering-rate path on B200.
+
+Workload (one GPU): the 16x16x16 diamond solve -- 2-atom cell, fcc a=5.43 A,
+masses 28.085 amu, seeded Born-von Karman springs and N(0,5)/N(0,2) cubic and
+quartic clusters (3rd-neighbour / 1st-neighbour cutoffs), T in {300, 700} K,
+scalebroad 1.  One step is one RTA_driver_4ph pass over all 870 irreducible
+modes with both temperatures fused (the matrix elements are contracted once
+and weighted for both).  Synthetic inputs generated from a fixed seed.
+
+Metric: four-phonon processes/s (surviving processes of the energy filter,
+counted as the reference's N_plusplus+N_plusminus+N_minusminus).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs one rank per GPU (torchrun); each rank solves the same cell at its
+own pair of temperatures (300+10r, 700+10r K): per-GPU work is fixed
+(weak scaling) and there is no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT,):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "4ph processes/s"
+UNIT = "processes/s"
+WORKLOAD = "diamond 2-atom fcc a=5.43A, 16x16x16 q-grid, 3ph+4ph, 4ph RTA at T={300,700}K fused, scalebroad=1"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", type=int, default=16, help="q-grid edge (16 = the benchmarked workload)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    return ap.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------- workload
+
+
+def workload(grid, rank=0):
+    from fourphonon_b200 import system as S
+
+    temps = (300.0 + 10.0 * rank, 700.0 + 10.0 * rank)
+    base = S.cached_solve("diamond", (grid, grid, grid), temperatures=(300.0, 700.0))
+    if rank:
+        import copy
+
+        s = copy.copy(base)
+        s.temperatures = list(temps)
+        return s
+    return base
+
+
+def ref_flops_per_process(s):
+    """The reference's per-process contraction work (SURVEY convention):
+    644*Ntri4 + 40 real flops (Vp_pp/pm/mm plus weights)."""
+    return 644.0 * s.ifc4.ntri + 40.0
+
+
+def executed_flops(s, counters, npi):
+    """FP64 operations the main kernel executes (see DESIGN: k4_work)."""
+    nproc, ncontr, nsig, ncand, nz = counters[:5]
+    nT = len(s.temperatures)
+    f_sigma = 27.0
+    f_test = 3.0
+    f_proc = 27.0 + 25.0 + 12.0 * nT + 116.0 * npi
+    f_z = s.nb * 9.0 * npi * 0 + s.nb * 9.0 * s.ifc4.ntri * 98.0  # per table build (one branch i, all j)
+    return nsig * f_sigma + ncand * f_test + ncontr * f_proc + nz * f_z
+
+
+def npi_of(s):
+    f = s.ifc4
+    keys = set()
+    for c in range(f.ntri):
+        keys.add((tuple(f.cells[1, c] - f.cells[2, c]), int(f.atoms[2, c]), int(f.atoms[3, c])))
+    return len(keys)
+
+
+# ---------------------------------------------------------------------------- clocks
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = []
+        mx = None
+        reasons = set()
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+            except (ValueError, IndexError):
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for n, v in zip(names, s[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [x for x in sm if mx and x > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- distributed plumbing
+
+
+def dist_setup(n):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def all_max(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def all_sum(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------- CPU baseline (oracle)
+
+
+def cpu_sample(s, target_s=15.0):
+    """Time the oracle (the C restatement of RTA_driver_4ph, OpenMP over modes)
+    on a bounded sample: modes of the second irreducible q-point onward, each
+    restricted to the q' points 2..1+n; the sample is sized to ~target_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    lib = O.lib()
+    threads = lib.fp4o_num_threads()
+    o = O.Oracle(s, T=s.temperatures[0])
+    nm = s.nmodes
+    mm0 = s.nb  # skip the Gamma point
+    nmodes = min(nm - mm0, max(threads, 1) * 2)
+    t0 = time.perf_counter()
+    n = o.rta4_sample(mm0, mm0 + nmodes, 1, 2)
+    dt = time.perf_counter() - t0
+    per_ii = max(dt, 1e-3)
+    nii = int(max(1, min(s.nptk, target_s / per_ii)))
+    t0 = time.perf_counter()
+    n = o.rta4_sample(mm0, mm0 + nmodes, 1, 1 + nii)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle RTA_driver_4ph restatement, {nmodes} modes x q' points 2..{1 + nii} "
+                      f"(all three channels, T={s.temperatures[0]:.0f} K): {n} processes in {dt:.1f} s",
+            "processes": n, "seconds": dt}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    s = workload(args.grid)
+    vals = []
+    for w in range(args.warmup):
+        cpu_sample(s, target_s=2.0)
+    samples = []
+    for k in range(args.steps):
+        r = cpu_sample(s, target_s=10.0)
+        samples.append(r)
+        vals.append(r["value"])
+    v = float(np.mean(vals))
+    total_s = sum(r["seconds"] for r in samples)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": samples[-1]["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": samples[-1]["cores"], "kind": "port",
+                             "sample": samples[-1]["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------- our arm
+
+
+def fp64_dgemm_peak(torch):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def time_steps(torch, ctx, s, steps, flush):
+    """Run `steps` RTA_driver_4ph calls on torch's current stream; returns per-step
+    device ms (CUDA events), main-kernel ms, processes, contracted and counters."""
+    out = []
+    for _ in range(steps):
+        flush.zero_()  # write a buffer larger than L2 between steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = ctx.rta_driver_4ph(s)
+        e1.record()
+        torch.cuda.synchronize()
+        nproc, ncontr, call_ms, kms, launches = ctx.stats()
+        out.append(dict(ms=e0.elapsed_time(e1), kms=kms, nproc=nproc, ncontr=ncontr, launches=launches,
+                        counters=ctx.counters(), rates=r))
+    return out
+
+
+def pinned_copy(torch, s):
+    """A shallow copy of the solve whose arrays live in pinned host memory."""
+    import copy
+
+    def pin(a, order):
+        t = torch.empty(a.size * a.itemsize, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype)
+        if order == "F":
+            v = v.reshape(a.shape, order="F")
+            v[...] = a
+        else:
+            v = v.reshape(a.shape)
+            v[...] = a
+        return v, t
+
+    p = copy.copy(s)
+    keep = []
+    p.energy, t1 = pin(np.asfortranarray(s.energy), "F")
+    p.velocity, t2 = pin(np.asfortranarray(s.velocity), "F")
+    p.eig, t3 = pin(np.asfortranarray(s.eig), "F")
+    ifc = copy.copy(s.ifc4)
+    ifc.phi, t4 = pin(np.ascontiguousarray(s.ifc4.phi), "C")
+    ifc.R, t5 = pin(np.ascontiguousarray(s.ifc4.R), "C")
+    ifc.atoms, t6 = pin(np.ascontiguousarray(s.ifc4.atoms), "C")
+    p.ifc4 = ifc
+    keep += [t1, t2, t3, t4, t5, t6]
+    p._pinned = keep
+    h2d = sum(x.numel() for x in keep) + s.nlist * 4 + s.nptk * 12 + 8 * len(s.temperatures)
+    return p, h2d
+
+
+def rta_kappa(ctx, s, rate_total, t):
+    """kappa_RTA = trace/3 of sum over branches, from per-mode total rates (device BTE kernels)."""
+    tau = np.zeros_like(rate_total)
+    nz = rate_total != 0
+    tau[nz] = 1.0 / rate_total[nz]
+    F = ctx.iteration0(s, tau)
+    k = ctx.tconduct(s, F, T=s.temperatures[t]).reshape(3, 3, s.nb).sum(axis=2)
+    return float(np.trace(k) / 3.0)
+
+
+def run_ours(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    from fourphonon_b200 import abi
+
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    # rank 0 builds (and caches) the synthetic solve first
+    if rank == 0:
+        s = workload(args.grid, rank)
+    barrier(world)
+    if rank != 0:
+        s = workload(args.grid, rank)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    ctx = abi.Context(dev, abi.FP4_PREC_FP64)
+    ctx.set_stream(stream.cuda_stream)
+    npi = npi_of(s)
+
+    for _ in range(args.warmup):
+        ctx.rta_driver_4ph(s)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = Clocks(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    barrier(world)
+    res = time_steps(torch, ctx, s, args.steps, flush)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    t_local = sum(r["ms"] for r in res) / 1e3
+    t_max = all_max(world, t_local)
+    nproc_local = sum(r["nproc"] for r in res)
+    nproc_all = all_sum(world, nproc_local)
+    value = nproc_all / t_max
+    kms = float(np.mean([r["kms"] for r in res]))
+    last = res[-1]
+    cnt = last["counters"]
+    fl = executed_flops(s, cnt, npi)
+    achieved = fl / (kms / 1e3) / 1e12
+    launches = sum(r["launches"] for r in res)
+
+    out = {}
+    # mixed precision (same workload, FP32 contraction)
+    if not args.no_mixed:
+        cmx = abi.Context(dev, abi.FP4_PREC_MIXED)
+        cmx.set_stream(stream.cuda_stream)
+        for _ in range(max(1, args.warmup)):
+            cmx.rta_driver_4ph(s)
+        torch.cuda.synchronize()
+        barrier(world)
+        rmx = time_steps(torch, cmx, s, args.steps, flush)
+        barrier(world)
+        tmx = all_max(world, sum(r["ms"] for r in rmx) / 1e3)
+        vmx = all_sum(world, sum(r["nproc"] for r in rmx)) / tmx
+        r3 = ctx.rta_driver(s)["rate"]
+        kerr = []
+        rate_err = []
+        for t in range(len(s.temperatures)):
+            r64 = last["rates"]["rate_4ph"][t]
+            rm = rmx[-1]["rates"]["rate_4ph"][t]
+            k64 = rta_kappa(ctx, s, r3 + r64, t)
+            kmx = rta_kappa(ctx, s, r3 + rm, t)
+            k64_4 = rta_kappa(ctx, s, r64, t)
+            kmx_4 = rta_kappa(ctx, s, rm, t)
+            kerr.append(max(abs(kmx - k64) / abs(k64), abs(kmx_4 - k64_4) / abs(k64_4)))
+            m = r64 > 1e-6 * r64.max()
+            rate_err.append(float(np.max(np.abs(rm[m] - r64[m]) / r64[m])))
+        out["mixed"] = {"value": vmx, "unit": UNIT, "speedup_vs_fp64": vmx / value, "kappa_rel_err": max(kerr),
+                        "rate_rel_err_max": max(rate_err), "dtype": "f32 contraction, f64 filter/weights/reductions",
+                        "kernel_ms": float(np.mean([r["kms"] for r in rmx]))}
+        cmx.close()
+
+    # end to end through the public API with host buffers (no upload cache)
+    if not args.no_e2e:
+        ce = abi.Context(dev, abi.FP4_PREC_FP64)
+        ce.set_stream(stream.cuda_stream)
+        ce.set_upload_cache(False)
+        ps, h2d = pinned_copy(torch, s)
+        d2h = 6 * s.nmodes * len(s.temperatures) * 8
+        ce.rta_driver_4ph(ps)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        n_e = 0
+        for _ in range(args.steps):
+            ce.rta_driver_4ph(ps)
+            n_e += ce.stats()[0]
+        torch.cuda.synchronize()
+        te = all_max(world, time.perf_counter() - t0)
+        barrier(world)
+        out["e2e"] = {"value": all_sum(world, n_e) / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                      "d2h_bytes_per_step": int(d2h)}
+        ce.close()
+
+    peak = fp64_dgemm_peak(torch) if rank == 0 else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(s, target_s=15.0)
+    ctx.close()
+    if rank != 0:
+        barrier(world)
+        return 0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "k4_work_diamond16.txt")
+    if os.path.exists(tf):
+        for line in open(tf):
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "temperatures_K": s.temperatures, "nmodes": s.nmodes,
+                   "ntri4": s.ifc4.ntri, "displacement_classes": npi, "processes_per_step": last["nproc"],
+                   "contracted_per_step": last["ncontr"], "l2": "256 MiB buffer written between timed steps",
+                   "parallelism": f"{world} rank(s), independent solves"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": "k4_work", "kernel_ms": kms,
+                     "peak_note": "FP64: cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe peak; no FP64 figure in "
+                                  "MEASURED_PEAKS)",
+                     "achieved_note": "executed FP64 flops of k4_work from its work counters / event-timed duration",
+                     "ref_equivalent_tflops": last["nproc"] * ref_flops_per_process(s) / (kms / 1e3) / 1e12},
+        "clocks": clk, "gpu_launches": launches,
+        "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
+    }
+    line.update(out)
+    print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,379 @@
+// Linearised-BTE sweep and thermal conductivity on the device.
+//
+// iteration (Src/iterations.f90:34-92) is an in-place Gauss-Seidel sweep:
+// modes are visited in the order (ll, i, kk) and each update reads F_n values
+// already overwritten earlier in the same sweep.  The device sweep keeps that
+// order exactly: one CTA walks the (ll, i, kk) steps in sequence and spreads
+// each step's sum over the mode's processes across its threads (a tree
+// reduction, so only the summation order inside one step differs from the
+// reference's left-to-right loop).  F_n stays in the Fortran layout
+// F_n(nbands,nptk,3).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/fourphonon_b200.h"
+#include "fp4_ctx.h"
+#include "fp4_internal.h"
+
+using namespace fp4;
+
+namespace {
+
+struct BteParams {
+    int nb, nptk, nlist, nsr;
+    const int* nequi;
+    const int* allequi;   // ALLEquiList(nsr, *) column-major
+    const int* typeofsym; // TypeofSymmetry(nsr, *)
+    const int* id_equi;   // ID_equi(nsr, nptk)
+    const double* symm;   // symmetrizers(3,3,nptk)
+    const int* n_plus;
+    const int* n_minus;
+    const long long* off_plus;
+    const long long* off_minus;
+    const int* i2p;
+    const int* i3p;
+    const int* i2m;
+    const int* i3m;
+    const double* gp;
+    const double* gm;
+    const double* energy;    // energy(nptk,nb)
+    const double* velocity;  // velocity(nptk,nb,3)
+    const double* tau_zero;  // tau_zero(nb,nlist)
+    double* F;               // F_n(nb,nptk,3)
+};
+
+__device__ __forceinline__ double& Fat(const BteParams& p, int b, int q, int d) {
+    return p.F[((size_t)d * p.nptk + q) * p.nb + b];
+}
+
+__global__ void __launch_bounds__(1024) k_sweep(BteParams p) {
+    __shared__ double red[3][32];
+    __shared__ double res[3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nb = p.nb;
+    for (int ll = 0; ll < p.nlist; ll++) {
+        for (int i = 0; i < nb; i++) {
+            const int mm = ll * nb + i;
+            const int np_ = p.n_plus[mm], nm_ = p.n_minus[mm];
+            const long long op = p.off_plus[mm], om = p.off_minus[mm];
+            for (int kk = 0; kk < p.nequi[ll]; kk++) {
+                const int qq = p.allequi[ll * p.nsr + kk] - 1;
+                const int sym = p.typeofsym[ll * p.nsr + kk] - 1;
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+                for (int x = threadIdx.x; x < np_ + nm_; x += blockDim.x) {
+                    const bool plus = x < np_;
+                    const long long o = plus ? op + x : om + (x - np_);
+                    const int x2 = (plus ? p.i2p : p.i2m)[o] - 1, x3 = (plus ? p.i3p : p.i3m)[o] - 1;
+                    const int j = x2 % nb, m2 = x2 / nb, k = x3 % nb, n3 = x3 / nb;
+                    const int qa = p.id_equi[(size_t)n3 * p.nsr + sym] - 1;
+                    const int qb = p.id_equi[(size_t)m2 * p.nsr + sym] - 1;
+                    const double g = (plus ? p.gp : p.gm)[o];
+                    double t0, t1, t2;
+                    if (plus) {
+                        t0 = g * (Fat(p, k, qa, 0) - Fat(p, j, qb, 0));
+                        t1 = g * (Fat(p, k, qa, 1) - Fat(p, j, qb, 1));
+                        t2 = g * (Fat(p, k, qa, 2) - Fat(p, j, qb, 2));
+                    } else {
+                        t0 = g * (Fat(p, k, qa, 0) + Fat(p, j, qb, 0)) * 5.e-1;
+                        t1 = g * (Fat(p, k, qa, 1) + Fat(p, j, qb, 1)) * 5.e-1;
+                        t2 = g * (Fat(p, k, qa, 2) + Fat(p, j, qb, 2)) * 5.e-1;
+                    }
+                    a0 += t0;
+                    a1 += t1;
+                    a2 += t2;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+                    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+                    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+                }
+                if (lane == 0) {
+                    red[0][warp] = a0;
+                    red[1][warp] = a1;
+                    red[2][warp] = a2;
+                }
+                __syncthreads();
+                if (warp == 0) {
+                    double b0 = lane < nwarp ? red[0][lane] : 0.0;
+                    double b1 = lane < nwarp ? red[1][lane] : 0.0;
+                    double b2 = lane < nwarp ? red[2][lane] : 0.0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        b0 += __shfl_down_sync(0xffffffffu, b0, o);
+                        b1 += __shfl_down_sync(0xffffffffu, b1, o);
+                        b2 += __shfl_down_sync(0xffffffffu, b2, o);
+                    }
+                    if (lane == 0) {
+                        const double tz = p.tau_zero[ll * nb + i];
+                        const size_t e = (size_t)i * p.nptk + qq, pl = (size_t)p.nptk * nb;
+                        const double w = p.energy[e];
+                        res[0] = tz * p.velocity[e] * w + tz * b0;
+                        res[1] = tz * p.velocity[e + pl] * w + tz * b1;
+                        res[2] = tz * p.velocity[e + 2 * pl] * w + tz * b2;
+                        Fat(p, i, qq, 0) = res[0];
+                        Fat(p, i, qq, 1) = res[1];
+                        Fat(p, i, qq, 2) = res[2];
+                    }
+                }
+                __syncthreads();
+                // F_n(:,qq,:) = transpose(matmul(symmetrizers(:,:,qq), transpose(F_n(:,qq,:))))
+                if (threadIdx.x < nb) {
+                    const int b = threadIdx.x;
+                    const double* Sq = p.symm + 9 * (size_t)qq;
+                    double x0 = Fat(p, b, qq, 0), x1 = Fat(p, b, qq, 1), x2 = Fat(p, b, qq, 2);
+                    double y[3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) y[a] = Sq[a] * x0 + Sq[a + 3] * x1 + Sq[a + 6] * x2;
+                    Fat(p, b, qq, 0) = y[0];
+                    Fat(p, b, qq, 1) = y[1];
+                    Fat(p, b, qq, 2) = y[2];
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+__global__ void k_iteration0(int nb, int nptk, int nlist, int nsr, const int* nequi, const int* allequi,
+                             const double* energy, const double* velocity, const double* tau_zero, double* F) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nlist * nb * nsr; x += gridDim.x * blockDim.x) {
+        int kk = x % nsr, rest = x / nsr, i = rest % nb, ll = rest / nb;
+        if (kk >= nequi[ll]) continue;
+        int qq = allequi[ll * nsr + kk] - 1;
+        size_t e = (size_t)i * nptk + qq, pl = (size_t)nptk * nb;
+        double tz = tau_zero[ll * nb + i], w = energy[e];
+        for (int d = 0; d < 3; d++) F[((size_t)d * nptk + qq) * nb + i] = tz * velocity[e + d * pl] * w;
+    }
+}
+
+__global__ void k_symmetrize(int nb, int nptk, const double* symm, double* F) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nb * nptk; x += gridDim.x * blockDim.x) {
+        int b = x % nb, q = x / nb;
+        const double* Sq = symm + 9 * (size_t)q;
+        double v[3];
+        for (int d = 0; d < 3; d++) v[d] = F[((size_t)d * nptk + q) * nb + b];
+        for (int a = 0; a < 3; a++) F[((size_t)a * nptk + q) * nb + b] = Sq[a] * v[0] + Sq[a + 3] * v[1] + Sq[a + 6] * v[2];
+    }
+}
+
+// TConduct (conductivity.f90:11-37): one CTA per branch, q >= 2, fixed-order tree sum.
+__global__ void k_tconduct(int nb, int nptk, double T, double scale, const double* energy, const double* velocity,
+                           const double* F, double* kappa, double* kmode) {
+    __shared__ double red[9][32];
+    const int jj = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    double acc[9];
+    for (int x = 0; x < 9; x++) acc[x] = 0.0;
+    const size_t pl = (size_t)nptk * nb;
+    for (int ii = 1 + threadIdx.x; ii < nptk; ii += blockDim.x) {
+        size_t e = (size_t)jj * nptk + ii;
+        double w = energy[e];
+        double f = 1.0 / (exp(hbar * w / kb / T) - 1.0);
+        double c = f * (f + 1) * w;
+        for (int d2 = 0; d2 < 3; d2++) {
+            double Fd = F[((size_t)d2 * nptk + ii) * nb + jj];
+            for (int d1 = 0; d1 < 3; d1++) {
+                double m = c * (velocity[e + d1 * pl] * Fd);
+                acc[d2 * 3 + d1] += m;
+                if (kmode) kmode[(((size_t)(d2 * 3 + d1)) * nb + jj) * nptk + ii] = scale * m;
+            }
+        }
+    }
+    for (int x = 0; x < 9; x++) {
+        double v = acc[x];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[x][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        double t = 0.0;
+        for (int w = 0; w < nwarp; w++) t += red[threadIdx.x][w];
+        kappa[threadIdx.x * nb + jj] = scale * t;  // ThConductivity(jj,d1,d2): [(d2*3+d1)*nb + jj]
+    }
+}
+
+}  // namespace
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return fp4_fail(c, FP4_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static int check_g(fp4_ctx* c, const fp4_globals* g) {
+    if (!g) return fp4_fail(c, FP4_E_ARG, "null globals");
+    for (int d = 0; d < 3; d++)
+        if (g->ngrid[d] < 1) return fp4_fail(c, FP4_E_ARG, "ngrid must be >0");
+    if (g->nbands < 3) return fp4_fail(c, FP4_E_ARG, "nbands must be >=3");
+    return FP4_OK;
+}
+
+extern "C" int fp4_iteration0(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
+                              const int32_t* allequi, int32_t nsr, const double* omega, const double* velocity,
+                              const double* tau_zero, double* f_n) {
+    if (!c) return FP4_E_ARG;
+    int r;
+    if ((r = check_g(c, g))) return r;
+    if (!nequi || !allequi || !omega || !velocity || !tau_zero || !f_n || nlist < 1 || nsr < 1)
+        return fp4_fail(c, FP4_E_ARG, "bad argument");
+    if ((r = fp4_begin(c))) return r;
+    const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2];
+    DevBuffer* B = c->b_bte;
+    if ((r = B[0].upload(c, nequi, nlist * sizeof(int))) || (r = B[1].upload(c, allequi, (size_t)nlist * nsr * sizeof(int))) ||
+        (r = B[2].upload(c, omega, (size_t)nptk * nb * sizeof(double))) ||
+        (r = B[3].upload(c, velocity, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[4].upload(c, tau_zero, (size_t)nlist * nb * sizeof(double))) ||
+        (r = B[5].reserve(c, (size_t)nptk * nb * 3 * sizeof(double))))
+        return r;
+    CK(cudaMemsetAsync(B[5].ptr, 0, (size_t)nptk * nb * 3 * sizeof(double), c->stream));
+    k_iteration0<<<256, 256, 0, c->stream>>>(nb, nptk, nlist, nsr, B[0].as<int>(), B[1].as<int>(), B[2].as<double>(),
+                                            B[3].as<double>(), B[4].as<double>(), B[5].as<double>());
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(f_n, B[5].ptr, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return fp4_end(c);
+}
+
+extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
+                             const int32_t* allequi, const int32_t* typeofsym, int32_t nsr, const int32_t* id_equi,
+                             const double* symmetrizers, const int32_t* n_plus, const int32_t* n_minus,
+                             int32_t ntotal_plus, int32_t ntotal_minus, const int32_t* i2p, const int32_t* i3p,
+                             const int32_t* i2m, const int32_t* i3m, const double* omega, const double* velocity,
+                             const double* gp, const double* gm, const double* tau_zero, double* f_n) {
+    if (!c) return FP4_E_ARG;
+    int r;
+    if ((r = check_g(c, g))) return r;
+    if (!nequi || !allequi || !typeofsym || !id_equi || !symmetrizers || !n_plus || !n_minus || !omega || !velocity ||
+        !tau_zero || !f_n || nlist < 1 || nsr < 1 || ntotal_plus < 0 || ntotal_minus < 0)
+        return fp4_fail(c, FP4_E_ARG, "bad argument");
+    if ((ntotal_plus && (!i2p || !i3p || !gp)) || (ntotal_minus && (!i2m || !i3m || !gm)))
+        return fp4_fail(c, FP4_E_ARG, "null process list");
+    const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2], nm = nb * nlist;
+    std::vector<long long> op(nm + 1, 0), om(nm + 1, 0);
+    for (int m = 0; m < nm; m++) {
+        op[m + 1] = op[m] + n_plus[m];
+        om[m + 1] = om[m] + n_minus[m];
+    }
+    if (op[nm] != ntotal_plus || om[nm] != ntotal_minus)
+        return fp4_fail(c, FP4_E_ARG, "sum(N_plus)/sum(N_minus) differ from Ntotal_plus/Ntotal_minus");
+    for (int q = 0; q < nptk * nsr; q++)
+        if (id_equi[q] < 1 || id_equi[q] > nptk) return fp4_fail(c, FP4_E_ARG, "ID_equi entry outside [1,nptk]");
+    if ((r = fp4_begin(c))) return r;
+    DevBuffer* B = c->b_bte;
+    if ((r = B[0].upload(c, nequi, nlist * sizeof(int))) || (r = B[1].upload(c, allequi, (size_t)nlist * nsr * sizeof(int))) ||
+        (r = B[2].upload(c, omega, (size_t)nptk * nb * sizeof(double))) ||
+        (r = B[3].upload(c, velocity, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[4].upload(c, tau_zero, (size_t)nlist * nb * sizeof(double))) ||
+        (r = B[5].upload(c, f_n, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[6].upload(c, typeofsym, (size_t)nlist * nsr * sizeof(int))) ||
+        (r = B[7].upload(c, id_equi, (size_t)nptk * nsr * sizeof(int))) ||
+        (r = B[8].upload(c, symmetrizers, (size_t)nptk * 9 * sizeof(double))))
+        return r;
+    // process lists: [n_plus|n_minus|off_plus|off_minus] and [i2p|i3p|i2m|i3m] and [gp|gm]
+    std::vector<unsigned char> meta((size_t)nm * 2 * sizeof(int) + (size_t)(nm + 1) * 2 * sizeof(long long));
+    memcpy(meta.data(), n_plus, nm * sizeof(int));
+    memcpy(meta.data() + nm * sizeof(int), n_minus, nm * sizeof(int));
+    memcpy(meta.data() + 2 * nm * sizeof(int), op.data(), (nm + 1) * sizeof(long long));
+    memcpy(meta.data() + 2 * nm * sizeof(int) + (nm + 1) * sizeof(long long), om.data(), (nm + 1) * sizeof(long long));
+    if ((r = B[9].upload(c, meta.data(), meta.size()))) return r;
+    const size_t tp = ntotal_plus, tm = ntotal_minus;
+    if ((r = B[10].reserve(c, (2 * tp + 2 * tm) * sizeof(int) + 64)) || (r = B[11].reserve(c, (tp + tm) * sizeof(double) + 64)))
+        return r;
+    int* L = B[10].as<int>();
+    double* G = B[11].as<double>();
+    if (tp) {
+        CK(cudaMemcpyAsync(L, i2p, tp * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(L + tp, i3p, tp * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(G, gp, tp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    if (tm) {
+        CK(cudaMemcpyAsync(L + 2 * tp, i2m, tm * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(L + 2 * tp + tm, i3m, tm * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(G + tp, gm, tm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    BteParams p{};
+    p.nb = nb;
+    p.nptk = nptk;
+    p.nlist = nlist;
+    p.nsr = nsr;
+    p.nequi = B[0].as<int>();
+    p.allequi = B[1].as<int>();
+    p.energy = B[2].as<double>();
+    p.velocity = B[3].as<double>();
+    p.tau_zero = B[4].as<double>();
+    p.F = B[5].as<double>();
+    p.typeofsym = B[6].as<int>();
+    p.id_equi = B[7].as<int>();
+    p.symm = B[8].as<double>();
+    const unsigned char* mb = static_cast<const unsigned char*>(B[9].ptr);
+    p.n_plus = reinterpret_cast<const int*>(mb);
+    p.n_minus = p.n_plus + nm;
+    p.off_plus = reinterpret_cast<const long long*>(mb + 2 * nm * sizeof(int));
+    p.off_minus = p.off_plus + nm + 1;
+    p.i2p = L;
+    p.i3p = L + tp;
+    p.i2m = L + 2 * tp;
+    p.i3m = L + 2 * tp + tm;
+    p.gp = G;
+    p.gm = G + tp;
+    k_sweep<<<1, 1024, 0, c->stream>>>(p);
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(f_n, B[5].ptr, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    B[5].key = 0;  // device copy now differs from the caller's previous F_n
+    return fp4_end(c);
+}
+
+extern "C" int fp4_symmetrize_fn(fp4_ctx* c, const fp4_globals* g, const double* symmetrizers, double* f_n) {
+    if (!c) return FP4_E_ARG;
+    int r;
+    if ((r = check_g(c, g))) return r;
+    if (!symmetrizers || !f_n) return fp4_fail(c, FP4_E_ARG, "null argument");
+    const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2];
+    if ((r = fp4_begin(c))) return r;
+    DevBuffer* B = c->b_bte;
+    if ((r = B[8].upload(c, symmetrizers, (size_t)nptk * 9 * sizeof(double))) ||
+        (r = B[5].upload(c, f_n, (size_t)nptk * nb * 3 * sizeof(double))))
+        return r;
+    k_symmetrize<<<256, 256, 0, c->stream>>>(nb, nptk, B[8].as<double>(), B[5].as<double>());
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(f_n, B[5].ptr, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    B[5].key = 0;
+    return fp4_end(c);
+}
+
+extern "C" int fp4_tconduct(fp4_ctx* c, const fp4_globals* g, double V, const double* omega, const double* velocity,
+                            const double* f_n, double* kappa, double* kmode) {
+    if (!c) return FP4_E_ARG;
+    int r;
+    if ((r = check_g(c, g))) return r;
+    if (!omega || !velocity || !f_n || !kappa || !(V > 0.0) || !(g->T > 0.0)) return fp4_fail(c, FP4_E_ARG, "bad argument");
+    const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2];
+    if ((r = fp4_begin(c))) return r;
+    DevBuffer* B = c->b_bte;
+    if ((r = B[2].upload(c, omega, (size_t)nptk * nb * sizeof(double))) ||
+        (r = B[3].upload(c, velocity, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[5].upload(c, f_n, (size_t)nptk * nb * 3 * sizeof(double))) || (r = c->b_out.reserve(c, nb * 9 * sizeof(double))))
+        return r;
+    double* km = nullptr;
+    if (kmode) {
+        if ((r = B[10].reserve(c, (size_t)nptk * nb * 9 * sizeof(double)))) return r;
+        km = B[10].as<double>();
+        CK(cudaMemsetAsync(km, 0, (size_t)nptk * nb * 9 * sizeof(double), c->stream));
+        B[10].key = 0;
+    }
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    // 1e21*hbar**2*ThConductivity/(kB*T*T*V*nptk), 1e21 a default-REAL literal
+    const double scale = (double)1e21f * (hbar * hbar) / (kb * g->T * g->T * V * nptk);
+    k_tconduct<<<nb, 256, 0, c->stream>>>(nb, nptk, g->T, scale, B[2].as<double>(), B[3].as<double>(),
+                                          B[5].as<double>(), c->b_out.as<double>(), km);
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(kappa, c->b_out.ptr, nb * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (kmode) CK(cudaMemcpyAsync(kmode, km, (size_t)nptk * nb * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return fp4_end(c);
+}

@@ -1,0 +1,79 @@
+// The opaque fp4_ctx of the C-ABI: one CUDA stream and the device-resident
+// copies of a solve (harmonic arrays, cluster tables, queues, outputs).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fourphonon_b200.h"
+#include "fp4_device.cuh"
+
+struct fp4_ctx;
+
+// Grow-only device buffer that remembers a hash of the bytes last uploaded,
+// so repeated calls with unchanged inputs skip the host-to-device copy.
+struct DevBuffer {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    uint64_t key = 0;
+    int reserve(fp4_ctx* c, size_t bytes);
+    int upload(fp4_ctx* c, const void* host, size_t bytes);
+    void release();
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+struct IfcTables {
+    DevBuffer phi, atoms, mj, mk, ml, mu, cl_start, cl_index, pi_d, blk_start;
+    fp4::DevIfc F{};
+    std::vector<DevBuffer*> list() { return {&phi, &atoms, &mj, &mk, &ml, &mu, &cl_start, &cl_index, &pi_d, &blk_start}; }
+};
+
+struct fp4_ctx {
+    int device = 0;
+    int sm_count = 148;
+    int precision = 0;
+    cudaStream_t stream = nullptr;      // stream in use (own or caller's)
+    cudaStream_t own_stream = nullptr;  // created with the context
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
+    bool upload_cache = true;
+    bool kernel_timed = false;
+    bool wv_packed = false;
+    uint64_t wv_key = 0;
+    int64_t launches = 0;
+    std::string err;
+    fp4::DevSys S{};
+    std::vector<double> atom_mass;
+    bool eig_packed = false;
+    DevBuffer b_energy, b_velocity, b_wv, b_eigraw, b_eig, b_eigf, b_list, b_root[3], b_rootf[3];
+    DevBuffer b_temps, b_bose, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
+    DevBuffer b_queue, b_part, b_work, b_err, b_stats;
+    DevBuffer b_bte[12];
+    IfcTables ifc3, ifc4;
+    int64_t last_nproc = 0, last_ncontr = 0, last_launches = 0;
+    int64_t last_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double last_ms = 0.0, last_kernel_ms = 0.0;
+    std::vector<DevBuffer*> all_buffers() {
+        std::vector<DevBuffer*> v = {&b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,
+                                     &b_temps,  &b_bose,     &b_out, &b_out4,   &b_lists, &b_gamma, &b_off,
+                                     &b_counts, &b_queue,    &b_part, &b_work,  &b_err,   &b_stats};
+        for (int d = 0; d < 3; d++) {
+            v.push_back(&b_root[d]);
+            v.push_back(&b_rootf[d]);
+        }
+        for (auto& b : b_bte) v.push_back(&b);
+        for (auto* b : ifc3.list()) v.push_back(b);
+        for (auto* b : ifc4.list()) v.push_back(b);
+        return v;
+    }
+};
+
+int fp4_fail(fp4_ctx* c, int code, const char* fmt, ...);
+int fp4_begin(fp4_ctx* c);
+int fp4_end(fp4_ctx* c);
+int fp4_setup_system(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
+                     const double* eigenvect, int32_t nlist, const int32_t* list, const int32_t* ijk);

@@ -1,0 +1,141 @@
+// Device-side data layout and arithmetic shared by the rate kernels.
+//
+// Layout in HBM (built once per system by the C-ABI layer):
+//   wv[q*nb + b]            double4 {vx, vy, vz, omega}: one 32-byte load per mode
+//   eig[(q*nb + b)*nb + c]  double2 eigenvector component c of mode (q,b)
+//   eigf[...]               float2 copy for the mixed-precision contraction
+//   bose[t*nptk*nb + q*nb + b]  Bose-Einstein occupation at temperature t
+//   root_d[x]               exp(2*pi*i*x/N_d), x in [0,N_d), per grid axis d
+// Clusters carry integer lattice coordinates of their cells, so every Bloch
+// phase exp(i q.R) is exp(2*pi*i*sum_d n_d m_d / N_d), looked up exactly in
+// the root tables instead of evaluating cos/sin of a rounded dot product.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fp4 {
+
+constexpr int kMaxNb = 32;       // nbands <= 32 (natoms <= 10)
+constexpr int kMaxTemps = 8;     // temperatures fused in one rate call
+constexpr int kMaxGrid = 64;     // ngrid(d) <= 64
+
+struct DevSys {
+    int n[3];
+    int nptk, nb, nlist, natoms;
+    double rl[9];  // rlattvec(3,3) column-major
+    double scalebroad, omega_max;
+    int onlyharmonic;
+    const double4* wv;
+    const double2* eig;
+    const float2* eigf;
+    const int* list0;  // 0-based q of irreducible point ll
+    const double2* root[3];
+    const float2* rootf[3];
+};
+
+struct DevIfc {
+    int order, ntri, npi, nblk;  // nblk = natoms^2 atom-pair blocks of the class table
+    const double* phi;           // per cluster 27 (3ph: [t][s][r]) or 81 (4ph: [u][t][s][r]) entries
+    const int4* atoms;           // 0-based (a1,a2,a3,a4)
+    const int4* mj;              // lattice coordinates of the 2nd atom's cell
+    const int4* mk;              // ... 3rd
+    const int4* ml;              // ... 4th (4ph)
+    const double* mu;            // 1/sqrt(product of masses)
+    const int* cl_start;         // clusters sorted by class: class p owns [cl_start[p], cl_start[p+1])
+    const int* cl_index;         // cluster ids in class order
+    const int4* pi_d;            // class displacement D (x,y,z) and packed atom pair in .w
+    const int* blk_start;        // classes sorted by atom-pair block: block b owns [blk_start[b], blk_start[b+1])
+};
+
+// ---------------------------------------------------------------------------
+// complex helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+    return acc;
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmacf(float2 acc, float2 a, float2 b) {
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+    return acc;
+}
+__device__ __forceinline__ float2 cconjf(float2 a) { return make_float2(a.x, -a.y); }
+
+__device__ __forceinline__ int pmod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// exp(2*pi*i * sum_d n_d*m_d/N_d): three table lookups, two complex products
+__device__ __forceinline__ double2 lattice_phase(const DevSys& S, int n0, int n1, int n2, int m0, int m1, int m2) {
+    double2 a = S.root[0][pmod(n0 * m0, S.n[0])];
+    double2 b = S.root[1][pmod(n1 * m1, S.n[1])];
+    double2 c = S.root[2][pmod(n2 * m2, S.n[2])];
+    return cmul(cmul(a, b), c);
+}
+__device__ __forceinline__ float2 lattice_phase_f(const DevSys& S, int n0, int n1, int n2, int m0, int m1, int m2) {
+    float2 a = S.rootf[0][pmod(n0 * m0, S.n[0])];
+    float2 b = S.rootf[1][pmod(n1 * m1, S.n[1])];
+    float2 c = S.rootf[2][pmod(n2 * m2, S.n[2])];
+    return cmulf(cmulf(a, b), c);
+}
+
+// q index <-> grid coordinates (Id2ind, config.f90:458-468; Index_N of processes.f90)
+__device__ __forceinline__ void q_coords(const DevSys& S, int q, int& a, int& b, int& c) {
+    a = q % S.n[0];
+    int t = q / S.n[0];
+    b = t % S.n[1];
+    c = t / S.n[1];
+}
+__device__ __forceinline__ int q_index(const DevSys& S, int a, int b, int c) { return (c * S.n[1] + b) * S.n[0] + a; }
+
+// ---------------------------------------------------------------------------
+// Energy-conservation filter, bit-exact with the reference's source order.
+// base_sigma (config.f90:481-499):  max over nu of
+//   ((rl(1,nu)*v1 + rl(2,nu)*v2) + rl(3,nu)*v3) / ngrid(nu), squared;
+// then sqrt(x/2) and the scalebroad factor.  Every product and sum is
+// rounded separately (no fused multiply-add), exactly as written.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sigma_exact(const DevSys& S, double4 a, double4 b) {
+    double v0 = __dadd_rn(a.x, -b.x);
+    double v1 = __dadd_rn(a.y, -b.y);
+    double v2 = __dadd_rn(a.z, -b.z);
+    double m = 0.0;
+#pragma unroll
+    for (int nu = 0; nu < 3; nu++) {
+        const double* r = S.rl + 3 * nu;
+        double dp = __dadd_rn(__dadd_rn(__dmul_rn(r[0], v0), __dmul_rn(r[1], v1)), __dmul_rn(r[2], v2));
+        double x = __ddiv_rn(dp, (double)S.n[nu]);
+        double x2 = __dmul_rn(x, x);
+        m = (nu == 0 || x2 > m) ? x2 : m;
+    }
+    return __dmul_rn(S.scalebroad, __dsqrt_rn(__dmul_rn(m, 0.5)));
+}
+
+// Occupation 1/(exp(hbar*w/kB/T)-1), with the reference's operation order.
+__device__ __forceinline__ double bose_of(double w, double T) {
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    return 1.0 / (exp(hbar * w / kb / T) - 1.0);
+}
+
+// 4-byte packed survivor (q'' index plus three branch indices) in a 64-bit word
+__device__ __forceinline__ unsigned long long pack4(int jj, int j, int k, int l) {
+    return ((unsigned long long)(unsigned)jj << 32) | ((unsigned)j << 16) | ((unsigned)k << 8) | (unsigned)l;
+}
+
+// Error flags raised by kernels (read back by the host after each call)
+enum : int { kErrQueue = 1, kErrTable = 2 };
+
+}  // namespace fp4

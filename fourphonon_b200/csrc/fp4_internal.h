@@ -1,0 +1,71 @@
+// Kernel parameter blocks and launch helpers shared by the .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fp4_device.cuh"
+
+namespace fp4 {
+
+constexpr int kQ3 = 2048;  // 3-phonon survivor queue (shared memory entries)
+
+struct P3Params {
+    DevSys S;
+    DevIfc F;
+    const double* bose;  // [q*nb+b] at T
+    double scale;        // hbarp*pi/4
+    double unit;         // 5.60626442 (REAL) * 1e8
+    // outputs, index 0 = absorption (+), 1 = emission (-)
+    int32_t* n_out[2];
+    double* p_out[2];
+    double* rate[2];
+    double* wp[2];
+    const int32_t* nlist_counts[2];  // N_plus/N_minus (Ind_only, Ind)
+    const long long* list_off[2];    // Naccum offsets
+    int32_t* ind2[2];
+    int32_t* ind3[2];
+    double* gamma[2];
+    unsigned long long* stats;
+    int* err;
+};
+
+struct P4Params {
+    DevSys S;
+    DevIfc F;
+    int nT;
+    const double* bose;  // [t][q*nb+b]
+    int nwork;
+    int* work_counter;
+    int ch_of_work[3];
+    unsigned long long* queue;  // per CTA nb*nb bins of subcap entries
+    int subcap;
+    double* part_rate;  // [work][t][i]
+    double* part_wp;
+    unsigned long long* n_count;  // NP: [ch][mode]
+    double* p_sum;                // NP: [ch][mode]
+    unsigned long long* stats;    // [0] surviving processes, [1] contracted
+    int* err;
+};
+
+struct P4OrderParams {
+    DevSys S;
+    int ch;
+    const long long* list_off;  // Naccum per mode
+    const long long* counts;    // N per mode
+    long long* ind2;
+    long long* ind3;
+    long long* ind4;
+    int* err;
+};
+
+// launchers (fp4_rates.cu / fp4_order.cu)
+cudaError_t launch_k3(int mode, const P3Params& p, int nmodes, cudaStream_t st);
+size_t k3_smem(int mode, const DevIfc& F, bool onlyharmonic);
+cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st);
+size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F);
+cudaError_t launch_k4_reduce(const P4Params& p, double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp,
+                             double* wp_pm, double* wp_mm, double rate_scale, cudaStream_t st);
+cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st);
+cudaError_t launch_bose(const DevSys& S, const double* T, int nT, double* bose, cudaStream_t st);
+
+}  // namespace fp4

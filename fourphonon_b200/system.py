@@ -205,3 +205,29 @@ def load_solve(path) -> Solve:
                  np.asfortranarray(z["eig"]), sym, wd, [float(t) for t in z["temperatures"]],
                  scalebroad=float(z["scalebroad"]), omega_max=float(z["omega_max"]), ifc3=ifcs.get("ifc3"),
                  ifc4=ifcs.get("ifc4"))
+
+
+_CACHE: dict = {}
+
+
+def cached_solve(kind: str = "diamond", ngrid=(4, 4, 4), temperatures=(300.0,), seed=None) -> Solve:
+    """Synthetic solve built once and cached in memory and under _build/solves
+    (rebuilt from the seed when the file is absent)."""
+    key = (kind, tuple(ngrid), tuple(temperatures), seed)
+    if key in _CACHE:
+        return _CACHE[key]
+    root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+    d = os.path.join(root, "_build", "solves")
+    os.makedirs(d, exist_ok=True)
+    fn = os.path.join(d, f"{kind}_{'x'.join(map(str, ngrid))}_{'-'.join(str(int(t)) for t in temperatures)}_{seed}.npz")
+    if os.path.exists(fn):
+        s = load_solve(fn)
+    else:
+        builder = {"diamond": diamond_solve, "zincblende": zincblende_solve, "layered": layered_solve}[kind]
+        kw = {} if seed is None else {"seed": seed}
+        s = builder(ngrid=tuple(ngrid), temperatures=tuple(temperatures), **kw)
+        tmp = fn + f".{os.getpid()}.tmp.npz"
+        save_solve(tmp, s)
+        os.replace(tmp, fn)
+    _CACHE[key] = s
+    return s

@@ -1,0 +1,228 @@
+/*
+ * fourphonon_b200.h -- C-ABI of the B200 scattering-rate path.
+ *
+ * Each entry point replaces one Fortran subroutine of FourPhonon's hot path
+ * and takes that subroutine's arguments in the same order, with the same
+ * meaning, types and column-major layouts (indices stored in arrays are
+ * 1-based, as in the reference).  The reference keeps the run parameters in
+ * module globals (Src/config.f90:9-47); here they travel in fp4_globals.
+ *
+ * Array layouts (Fortran column-major):
+ *   energy(nptk,nbands)             double, rad/ps
+ *   velocity(nptk,nbands,3)         double, km/s
+ *   eigenvect(nptk,nbands,nbands)   double complex (re,im interleaved)
+ *   List(nlist), IJK(3,nptk)        int32
+ *   Phi(3,3,3,Ntri), R_j(3,Ntri)    double (eV/A^3, nm), Index_*(Ntri) int32
+ *   Psi(3,3,3,3,Ntri)               double (eV/A^4)
+ *   rate(nbands,nlist)              double, THz
+ *   N_plus(nlist*nbands) int32, N_plusplus(nlist*nbands) int64
+ *
+ * Every entry returns FP4_OK (0) or a negative FP4_E* code; the message of
+ * the last failure on a context is returned by fp4_last_error().  Calls on
+ * one context are not re-entrant (the reference calls them from the MPI main
+ * thread); distinct contexts are independent.  All arrays are caller-owned
+ * host memory; device copies are owned by the context.
+ */
+#ifndef FOURPHONON_B200_H
+#define FOURPHONON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FP4_OK 0
+#define FP4_E_ARG (-1)      /* bad shape / value / null pointer */
+#define FP4_E_CUDA (-2)     /* CUDA runtime error (no device, launch failure...) */
+#define FP4_E_CAPACITY (-3) /* a device work queue or table limit was exceeded */
+#define FP4_E_TIMEOUT (-4)  /* a bounded device wait gave up */
+#define FP4_E_STATE (-5)    /* call order (e.g. no system set) */
+
+#define FP4_PREC_FP64 0  /* all-FP64 drop-in */
+#define FP4_PREC_MIXED 1 /* FP32 contraction, FP64 filter/weights/reductions */
+
+typedef struct fp4_ctx fp4_ctx;
+
+/* Run parameters held by module globals in the reference (config.f90:9-47). */
+typedef struct {
+    int32_t ngrid[3];     /* ngrid */
+    int32_t nbands;       /* nbands = 3*natoms */
+    double rlattvec[9];   /* rlattvec(3,3), column-major, nm^-1 */
+    double T;             /* K */
+    double scalebroad;    /* scalebroad */
+    double omega_max;     /* omega_max (rad/ps) */
+    int32_t onlyharmonic; /* logical onlyharmonic */
+    int32_t nelements;    /* size of masses */
+    int32_t natoms;       /* size of types */
+    const double *masses; /* masses(nelements), amu */
+    const int32_t *types; /* types(natoms), 1-based */
+} fp4_globals;
+
+/* Context on CUDA device `device` (-1: current device). */
+int fp4_create(fp4_ctx **ctx, int device);
+int fp4_destroy(fp4_ctx *ctx);
+const char *fp4_last_error(const fp4_ctx *ctx);
+/* FP4_PREC_FP64 (default) or FP4_PREC_MIXED for the rate drivers. */
+int fp4_set_precision(fp4_ctx *ctx, int precision);
+
+/*
+ * Replaces NP_driver (Src/processes.f90:983-1067): per-mode counts of
+ * allowed 3-phonon processes and their phase-space volumes.
+ * Outputs N_plus(nlist*nbands), Pspace_plus_total(nbands,nlist), ...
+ */
+int fp4_np_driver(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity, int32_t nlist,
+                  const int32_t *list, const int32_t *ijk, int32_t *n_plus, double *pspace_plus, int32_t *n_minus,
+                  double *pspace_minus);
+
+/* Replaces NP_driver_4ph (Src/processes.f90:2749-2847). */
+int fp4_np_driver_4ph(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                      int32_t nlist, const int32_t *list, const int32_t *ijk, int64_t *n_plusplus,
+                      double *pspace_plusplus, int64_t *n_plusminus, double *pspace_plusminus, int64_t *n_minusminus,
+                      double *pspace_minusminus);
+
+/*
+ * Replaces Ind_only_driver (Src/processes.f90:1198-1309): the 3-phonon index
+ * lists Indof2ndPhonon_*(Ntotal), Indof3rdPhonon_*(Ntotal) in the
+ * reference's order (per mode: j outer, q' inner, k innermost) at the Naccum
+ * offsets of N_plus/N_minus (which the caller obtained from fp4_np_driver).
+ */
+int fp4_ind_only_driver(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                        int32_t nlist, const int32_t *list, const int32_t *ijk, const int32_t *n_plus,
+                        const int32_t *n_minus, int32_t *ind2_plus, int32_t *ind3_plus, int32_t *ind2_minus,
+                        int32_t *ind3_minus);
+
+/*
+ * Replaces Ind_only_driver_4ph (Src/processes.f90:3080-3246): the 4-phonon
+ * index lists (int64) in the reference's order (per mode: q', q'', j, k, l).
+ * Sized by N_plusplus etc.; meant for grids whose lists fit in host memory.
+ */
+int fp4_ind_only_driver_4ph(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                            int32_t nlist, const int32_t *list, const int32_t *ijk, const int64_t *n_plusplus,
+                            const int64_t *n_plusminus, const int64_t *n_minusminus, int64_t *ind2_pp,
+                            int64_t *ind3_pp, int64_t *ind4_pp, int64_t *ind2_pm, int64_t *ind3_pm,
+                            int64_t *ind4_pm, int64_t *ind2_mm, int64_t *ind3_mm, int64_t *ind4_mm);
+
+/*
+ * Replaces RTA_driver (Src/processes.f90:1676-1775) and its GPU twin
+ * RTA_driver_GPU_using_Ind (1778-1836): 3-phonon RTA rates at g->T.
+ * rate_minus carries the driver's factor 1/2; rate = rate_plus + rate_minus.
+ */
+int fp4_rta_driver(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                   const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk, int32_t ntri,
+                   const double *phi, const double *r_j, const double *r_k, const int32_t *index_i,
+                   const int32_t *index_j, const int32_t *index_k, double *rate, double *rate_plus,
+                   double *rate_minus, double *wp3_plus, double *wp3_minus);
+
+/*
+ * Replaces RTA_driver_4ph (Src/processes.f90:5174-5311) and its GPU twin
+ * RTA_driver_4ph_GPU_using_Ind (5315-5387): 4-phonon RTA rates at g->T.
+ * No index list is materialised: processes are enumerated, filtered and
+ * contracted on the device.
+ */
+int fp4_rta_driver_4ph(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                       const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk, int32_t ntri,
+                       const double *psi, const double *r_j, const double *r_k, const double *r_l,
+                       const int32_t *index_i, const int32_t *index_j, const int32_t *index_k,
+                       const int32_t *index_l, double *rate_4ph, double *rate_plusplus, double *rate_plusminus,
+                       double *rate_minusminus, double *wp4_plusplus, double *wp4_plusminus, double *wp4_minusminus);
+
+/*
+ * Multi-temperature form of fp4_rta_driver_4ph: the matrix elements are
+ * temperature independent, so they are contracted once and weighted for all
+ * nT temperatures (the reference re-runs RTA_driver_4ph per temperature in
+ * the loop of Src/ShengBTE.f90:787-1008).  g->T is ignored; outputs are
+ * (nbands,nlist,nT).
+ */
+int fp4_rta_driver_4ph_multi_t(fp4_ctx *ctx, const fp4_globals *g, int32_t nT, const double *temperatures,
+                               const double *energy, const double *velocity, const double *eigenvect, int32_t nlist,
+                               const int32_t *list, const int32_t *ijk, int32_t ntri, const double *psi,
+                               const double *r_j, const double *r_k, const double *r_l, const int32_t *index_i,
+                               const int32_t *index_j, const int32_t *index_k, const int32_t *index_l,
+                               double *rate_plusplus, double *rate_plusminus, double *rate_minusminus,
+                               double *wp4_plusplus, double *wp4_plusminus, double *wp4_minusminus);
+
+/*
+ * Replaces Ind_driver (Src/processes.f90:524-707): per-process 3-phonon
+ * scattering amplitudes Gamma_plus/Gamma_minus with their index lists in the
+ * reference's order at the Naccum offsets of N_plus/N_minus, and the per-mode
+ * rates (rate_minus with the factor 1/2, Gamma_minus without it).
+ */
+int fp4_ind_driver(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                   const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk,
+                   const int32_t *n_plus, const int32_t *n_minus, int32_t ntri, const double *phi,
+                   const double *r_j, const double *r_k, const int32_t *index_i, const int32_t *index_j,
+                   const int32_t *index_k, int32_t *ind2_plus, int32_t *ind3_plus, double *gamma_plus,
+                   int32_t *ind2_minus, int32_t *ind3_minus, double *gamma_minus, double *rate, double *rate_plus,
+                   double *rate_minus, double *wp3_plus, double *wp3_minus);
+
+/*
+ * Replaces iteration0 (Src/iterations.f90:13-30).
+ * allequilist(nsymm_rot,*) as ALLEquiList; F_n(nbands,nptk,3).
+ */
+int fp4_iteration0(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32_t *nequi,
+                   const int32_t *allequilist, int32_t nsymm_rot, const double *omega, const double *velocity,
+                   const double *tau_zero, double *f_n);
+
+/*
+ * Replaces iteration (Src/iterations.f90:34-92): one Gauss-Seidel sweep of
+ * the linearised BTE over the 3-phonon lists, F_n updated in place (same
+ * sweep order), followed by no symmetrisation (the caller's loop applies it,
+ * see fp4_symmetrize_fn).  id_equi(nsymm_rot,nptk) is symmetry_map's table
+ * (Src/config.f90:397-419), symmetrizers(3,3,nptk).
+ */
+int fp4_iteration(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32_t *nequi,
+                  const int32_t *allequilist, const int32_t *typeofsymmetry, int32_t nsymm_rot,
+                  const int32_t *id_equi, const double *symmetrizers, const int32_t *n_plus, const int32_t *n_minus,
+                  int32_t ntotal_plus, int32_t ntotal_minus, const int32_t *ind2_plus, const int32_t *ind3_plus,
+                  const int32_t *ind2_minus, const int32_t *ind3_minus, const double *omega,
+                  const double *velocity, const double *gamma_plus, const double *gamma_minus,
+                  const double *tau_zero, double *f_n);
+
+/* F_n(:,q,:) symmetrisation of every q (Src/ShengBTE.f90:1288-1290). */
+int fp4_symmetrize_fn(fp4_ctx *ctx, const fp4_globals *g, const double *symmetrizers, double *f_n);
+
+/*
+ * Replaces TConduct (Src/conductivity.f90:11-37).  V: unit-cell volume, nm^3.
+ * thconductivity(nbands,3,3); thconductivitymode(nptk,nbands,3,3) may be NULL.
+ */
+int fp4_tconduct(fp4_ctx *ctx, const fp4_globals *g, double V, const double *omega, const double *velocity,
+                 const double *f_n, double *thconductivity, double *thconductivitymode);
+
+/*
+ * Statistics of the last call on the context: surviving processes (all
+ * channels), processes whose matrix element was contracted (the others have
+ * a zero weight, w<=1.25 rad/ps), the device time of the whole call and of
+ * its main rate kernel in milliseconds, and the number of kernel launches.
+ * Any output pointer may be NULL.
+ */
+int fp4_last_stats(const fp4_ctx *ctx, int64_t *n_processes, int64_t *n_contracted, double *call_ms,
+                   double *kernel_ms, int64_t *launches);
+
+/*
+ * Work counters of the last four-phonon call: [0] surviving processes,
+ * [1] contracted processes, [2] broadening evaluations (one per (q'',k,l)
+ * candidate triple), [3] energy tests in the sorted windows, [4] reciprocal
+ * cluster tables built, [5..7] reserved (0).
+ */
+int fp4_last_counters(const fp4_ctx *ctx, int64_t counters[8]);
+
+/*
+ * Run the context's work on an existing CUDA stream (a cudaStream_t passed
+ * as void*); NULL restores the context's own stream.  Not part of the
+ * reference interface: lets a host that owns a stream order these calls
+ * with its own work.
+ */
+int fp4_set_stream(fp4_ctx *ctx, void *stream);
+
+/*
+ * Device copies of unchanged inputs are reused between calls (enable=1,
+ * default); enable=0 copies every input on every call.
+ */
+int fp4_set_upload_cache(fp4_ctx *ctx, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -451,6 +451,7 @@ typedef struct {
     double P, gamma, wp;
     int64_t cap;
     int64_t *ind2, *ind3, *ind4;
+    int ii0, ii1; /* optional q' range [ii0, ii1) (0-based); ii1 == 0 means all */
 } acc4_t;
 
 static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int mode, acc4_t *a) {
@@ -467,8 +468,9 @@ static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int 
     a->wp = 0.0;
     const double floor_sigma = (double)0.001f;
     const double pdenom = (double)nptk * (double)nptk * (double)nptk;
+    int ii_lo = (a->ii1 > 0) ? a->ii0 + 1 : 1, ii_hi = (a->ii1 > 0) ? a->ii1 : nptk;
     if (omega != 0) {
-        for (int ii = 1; ii <= nptk; ii++) {
+        for (int ii = ii_lo; ii <= ii_hi; ii++) {
             int jj0 = (ch == 1) ? 1 : ii;
             for (int jj = jj0; jj <= nptk; jj++) {
                 int qp[3], qdp[3], qtp[3];
@@ -606,6 +608,29 @@ void fp4o_rta4(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, double *r
         rate_mm[m0] = a.gamma;
         wp_mm[m0] = a.wp;
     }
+}
+
+/*
+ * Bounded sample of RTA_driver_4ph for timing: modes [mm0,mm1), each
+ * restricted to the q' range [ii0,ii1).  Returns the number of surviving
+ * processes visited; rates are not normalised (timing use only).
+ */
+int64_t fp4o_rta4_sample(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int ii0, int ii1) {
+    int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
+    for (int m0 = mm0; m0 < mm1; m0++) {
+        int mm = m0 + 1;
+        if (!gate(s, mm)) continue;
+        for (int ch = 0; ch < 3; ch++) {
+            acc4_t a;
+            memset(&a, 0, sizeof a);
+            a.ii0 = ii0;
+            a.ii1 = ii1;
+            proc4_one(s, f, mm, ch, 2, &a);
+            total += a.n;
+        }
+    }
+    return total;
 }
 
 /* ------------------------------------------------------------------------- */

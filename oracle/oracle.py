@@ -44,6 +44,7 @@ def lib():
         _lib.fp4o_ind_only3.restype = ct.c_int64
         _lib.fp4o_ind_only4.restype = ct.c_int64
         _lib.fp4o_num_threads.restype = ct.c_int
+        _lib.fp4o_rta4_sample.restype = ct.c_int64
     return _lib
 
 
@@ -142,6 +143,11 @@ class Oracle:
         out = [np.zeros(nm) for _ in range(6)]
         lib().fp4o_rta4(ct.byref(self.sys), ct.byref(self.ifc4), mm0, mm1, *[_p(x) for x in out])
         return out  # rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm
+
+    def rta4_sample(self, mm0, mm1, ii0, ii1):
+        """Timing sample: RTA_driver_4ph work for modes [mm0,mm1) restricted to
+        q' in [ii0,ii1); returns the number of surviving processes visited."""
+        return int(lib().fp4o_rta4_sample(ct.byref(self.sys), ct.byref(self.ifc4), mm0, mm1, ii0, ii1))
 
     def ind3(self, n_plus, n_minus):
         tp, tm = int(n_plus.sum()), int(n_minus.sum())

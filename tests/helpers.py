@@ -52,24 +52,5 @@ class GoldenSolve:
                 np.asfortranarray(self.eig).ravel(order="F"))
 
 
-_CACHE = {}
-
-
 def cached_solve(kind="diamond", ngrid=(4, 4, 4), temperatures=(300.0,), seed=None):
-    """Synthetic solves, built once per process and cached on disk under
-    _build/solves (regenerated if missing)."""
-    key = (kind, tuple(ngrid), tuple(temperatures), seed)
-    if key in _CACHE:
-        return _CACHE[key]
-    d = os.path.join(ROOT, "_build", "solves")
-    os.makedirs(d, exist_ok=True)
-    fn = os.path.join(d, f"{kind}_{'x'.join(map(str, ngrid))}_{'-'.join(str(int(t)) for t in temperatures)}_{seed}.npz")
-    if os.path.exists(fn):
-        s = S.load_solve(fn)
-    else:
-        builder = {"diamond": S.diamond_solve, "zincblende": S.zincblende_solve, "layered": S.layered_solve}[kind]
-        kw = {} if seed is None else {"seed": seed}
-        s = builder(ngrid=ngrid, temperatures=temperatures, **kw)
-        S.save_solve(fn, s)
-    _CACHE[key] = s
-    return s
+    return S.cached_solve(kind, ngrid, temperatures, seed)

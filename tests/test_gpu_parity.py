@@ -1,0 +1,252 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Bars: process counts and index lists bit-exact; FP64 rates within 1e-10
+relative; mixed-precision kappa within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+import oracle as O
+from fourphonon_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-10
+RTOL_MIXED_KAPPA = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = abi.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def s4():
+    return H.cached_solve("diamond", (4, 4, 4))
+
+
+@pytest.fixture(scope="module")
+def s6():
+    return H.cached_solve("diamond", (6, 6, 6), temperatures=(300.0, 700.0))
+
+
+def close(a, b, rtol):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.abs(b).max() if b.size else 0.0
+    err = np.abs(a - b)
+    ok = err <= rtol * np.abs(b) + 1e-3 * rtol * scale
+    return bool(ok.all()), float((err / np.maximum(np.abs(b), 1e-300)).max() if b.size else 0.0)
+
+
+# ---------------------------------------------------------------------------- counts and lists
+
+
+def test_np3_counts_bit_exact(ctx, s6):
+    g = ctx.np_driver(s6)
+    o = O.Oracle(s6).np3()
+    assert np.array_equal(g[0], o[0]) and np.array_equal(g[1], o[1])
+    for a, b in ((g[2], o[2]), (g[3], o[3])):
+        ok, e = close(a, b, 1e-12)
+        assert ok, e
+
+
+def test_ind_only3_lists_bit_exact(ctx, s6):
+    n_p, n_m, _, _ = ctx.np_driver(s6)
+    a, b, c, d = ctx.ind_only_driver(s6, n_p, n_m)
+    o = O.Oracle(s6)
+    off_p = np.concatenate([[0], np.cumsum(n_p)])
+    off_m = np.concatenate([[0], np.cumsum(n_m)])
+    for m in range(s6.nmodes):
+        if n_p[m]:
+            x2, x3, n = o.ind_only3(m + 1, 1, int(n_p[m]) + 8)
+            assert n == n_p[m]
+            assert np.array_equal(a[off_p[m]:off_p[m + 1]], x2) and np.array_equal(b[off_p[m]:off_p[m + 1]], x3)
+        if n_m[m]:
+            x2, x3, n = o.ind_only3(m + 1, -1, int(n_m[m]) + 8)
+            assert n == n_m[m]
+            assert np.array_equal(c[off_m[m]:off_m[m + 1]], x2) and np.array_equal(d[off_m[m]:off_m[m + 1]], x3)
+
+
+@pytest.mark.parametrize("grid", [(4, 4, 4), (6, 6, 6)])
+def test_np4_counts_bit_exact(ctx, grid):
+    s = H.cached_solve("diamond", grid)
+    n, p = ctx.np_driver_4ph(s)
+    on, op = O.Oracle(s).np4()
+    for ch in range(3):
+        assert np.array_equal(n[ch], on[ch]), (ch, int(n[ch].sum()), int(on[ch].sum()))
+        ok, e = close(p[ch], op[ch], 1e-11)
+        assert ok, (ch, e)
+
+
+def test_ind_only4_lists_bit_exact(ctx, s4):
+    n, _ = ctx.np_driver_4ph(s4)
+    lists = ctx.ind_only_driver_4ph(s4, *n)
+    o = O.Oracle(s4)
+    for ch in range(3):
+        off = np.concatenate([[0], np.cumsum(n[ch])])
+        for m in range(s4.nmodes):
+            if n[ch][m] == 0:
+                continue
+            a, b, c, cnt = o.ind_only4(m + 1, ch, int(n[ch][m]) + 8)
+            assert cnt == n[ch][m]
+            sl = slice(off[m], off[m + 1])
+            assert np.array_equal(lists[ch][0][sl], a)
+            assert np.array_equal(lists[ch][1][sl], b)
+            assert np.array_equal(lists[ch][2][sl], c)
+
+
+# ---------------------------------------------------------------------------- rates
+
+
+def test_rta3_rates_fp64(ctx, s6):
+    g = ctx.rta_driver(s6)
+    rp, rm, wpp, wpm = O.Oracle(s6).rta3()
+    for a, b in ((g["rate_plus"], rp), (g["rate_minus"], rm), (g["wp3_plus"], wpp), (g["wp3_minus"], wpm)):
+        ok, e = close(a, b, RTOL_FP64)
+        assert ok, e
+
+
+def test_rta4_rates_fp64_all_modes(ctx, s4):
+    g = ctx.rta_driver_4ph(s4)
+    o = O.Oracle(s4).rta4()
+    names = ("rate_plusplus", "rate_plusminus", "rate_minusminus", "wp4_plusplus", "wp4_plusminus", "wp4_minusminus")
+    for name, ref in zip(names, o):
+        ok, e = close(g[name][0], ref, RTOL_FP64)
+        assert ok, (name, e)
+
+
+def test_rta4_rates_fp64_two_temperatures(ctx, s6):
+    g = ctx.rta_driver_4ph(s6)  # T = 300, 700 fused
+    mm0, mm1 = 6, 18  # irreducible q-points 2 and 3
+    for t, T in enumerate(s6.temperatures):
+        o = O.Oracle(s6, T=T).rta4(mm0, mm1)
+        for ch, name in enumerate(("rate_plusplus", "rate_plusminus", "rate_minusminus")):
+            ok, e = close(g[name][t][mm0:mm1], o[ch][mm0:mm1], RTOL_FP64)
+            assert ok, (T, name, e)
+
+
+def test_ind_driver_lists_and_gamma(ctx, s6):
+    n_p, n_m, _, _ = ctx.np_driver(s6)
+    g = ctx.ind_driver(s6, n_p, n_m)
+    o = O.Oracle(s6).ind3(n_p, n_m)
+    for k in ("ind2_plus", "ind3_plus", "ind2_minus", "ind3_minus"):
+        assert np.array_equal(g[k], o[k]), k
+    for k in ("gamma_plus", "gamma_minus", "rate_plus", "rate_minus", "wp3_plus", "wp3_minus"):
+        ok, e = close(g[k], o[k], RTOL_FP64)
+        assert ok, (k, e)
+
+
+# ---------------------------------------------------------------------------- BTE and kappa
+
+
+def _tau_zero(rate):
+    t = np.zeros_like(rate)
+    nz = rate != 0
+    t[nz] = 1.0 / rate[nz]
+    return t
+
+
+def test_iteration_and_kappa(ctx, s6):
+    """Three sweeps of the Gauss-Seidel BTE plus TConduct, device vs oracle."""
+    n_p, n_m, _, _ = ctx.np_driver(s6)
+    lists = O.Oracle(s6).ind3(n_p, n_m)
+    rate = lists["rate_plus"] + lists["rate_minus"]
+    tau = _tau_zero(rate)
+    o = O.Oracle(s6)
+    Fg = ctx.iteration0(s6, tau)
+    Fo = o.iteration0(tau)
+    assert np.array_equal(Fg, Fo)
+    for it in range(3):
+        Fg = ctx.iteration(s6, Fg, tau, n_p, n_m, lists)
+        Fg = ctx.symmetrize_fn(s6, Fg)
+        Fo = o.iteration(Fo, tau, n_p, n_m, lists)
+        Fo = o.symmetrize_fn(Fo)
+        ok, e = close(Fg, Fo, 1e-9)
+        assert ok, (it, e)
+    kg = ctx.tconduct(s6, Fg)
+    ko = o.tconduct(Fo)
+    ok, e = close(kg, ko, 1e-9)
+    assert ok, e
+
+
+# ---------------------------------------------------------------------------- mixed precision
+
+
+def _rta_kappa(s, rate_total, tconduct):
+    """kappa_RTA (sum over branches, trace/3) from per-mode total rates."""
+    tau = _tau_zero(rate_total)
+    o = O.Oracle(s)
+    F = o.iteration0(tau)
+    k = tconduct(F).reshape(3, 3, s.nb).sum(axis=2)
+    return np.trace(k) / 3.0
+
+
+def test_mixed_path_kappa_within_1e_4(s6):
+    c64 = abi.Context(0, abi.FP4_PREC_FP64)
+    cmx = abi.Context(0, abi.FP4_PREC_MIXED)
+    try:
+        r64 = c64.rta_driver_4ph(s6)
+        rmx = cmx.rta_driver_4ph(s6)
+        r3 = c64.rta_driver(s6)["rate"]
+        o = O.Oracle(s6)
+        for t in range(len(s6.temperatures)):
+            # kappa with 3ph+4ph rates, and with the 4ph rates alone (where the mixed path acts)
+            for base in (r3, 0.0 * r3):
+                k64 = _rta_kappa(s6, base + r64["rate_4ph"][t], o.tconduct)
+                kmx = _rta_kappa(s6, base + rmx["rate_4ph"][t], o.tconduct)
+                assert abs(kmx - k64) <= RTOL_MIXED_KAPPA * abs(k64), (k64, kmx)
+            rel = np.abs(rmx["rate_4ph"][t] - r64["rate_4ph"][t]) / np.maximum(np.abs(r64["rate_4ph"][t]), 1e-300)
+            assert np.nanmax(np.where(r64["rate_4ph"][t] > 1e-6 * r64["rate_4ph"][t].max(), rel, 0)) < 1e-3
+    finally:
+        c64.close()
+        cmx.close()
+
+
+# ---------------------------------------------------------------------------- reference golden data
+
+
+def test_golden_licoo2_4ph_counts(ctx):
+    """Four-phonon counts of the whole LiCoO2 10^3 example against its log.out
+    totals and BTE.Numprocess_4ph.  The inputs are the reference's printed
+    omega/v (10 digits), so candidates within that rounding of the threshold
+    may flip: totals agree to a few 1e-6, per-mode counts to 2e-5."""
+    g = H.GoldenSolve("LiCoO2")
+    n, p = ctx.np_driver_4ph(g)
+    tot = [int(x.sum()) for x in n]
+    ref = [int(x) for x in g.z["ntotal_4ph"]]
+    for a, b in zip(tot, ref):
+        assert abs(a - b) <= max(16, 5e-6 * b), (tot, ref)
+    gold = g.z["numprocess_4ph"]
+    for ch in range(3):
+        d = np.abs(n[ch] - gold[:, ch])
+        nz = gold[:, ch] > 0
+        exact = float(np.mean(d[nz] == 0)) if nz.any() else 1.0
+        rel = float((d[nz] / gold[nz, ch]).max()) if nz.any() else 0.0
+        assert exact >= 0.9 and rel <= 1e-3, (ch, exact, rel)
+        assert (d[~nz] == 0).all()
+    # and the device counts equal the oracle's on a slice of modes, bit for bit
+    on, _ = O.Oracle(g).np4(16, 18)
+    for ch in range(3):
+        assert np.array_equal(n[ch][16:18], on[ch][16:18])
+
+
+# ---------------------------------------------------------------------------- errors
+
+
+def test_bad_inputs_raise(ctx, s4):
+    import copy
+
+    s = copy.copy(s4)
+    s.wedge = copy.copy(s4.wedge)
+    s.wedge.list = s4.wedge.list.copy()
+    s.wedge.list[0] = s4.nptk + 5
+    with pytest.raises(abi.FP4Error) as ei:
+        ctx.np_driver(s)
+    assert ei.value.code == -1
+    # context still usable afterwards
+    n, _, _, _ = ctx.np_driver(s4)
+    assert n.sum() > 0
