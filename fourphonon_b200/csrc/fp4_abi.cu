@@ -228,6 +228,10 @@ int fp4_setup_system(fp4_ctx* c, const fp4_globals* g, const double* energy, con
     S.nlist = nlist;
     S.natoms = g->natoms;
     for (int x = 0; x < 9; x++) S.rl[x] = g->rlattvec[x];
+    for (int d = 0; d < 3; d++) {
+        S.ngd[d] = (double)g->ngrid[d];
+        S.rinv[d] = 1.0 / (double)g->ngrid[d];
+    }
     S.scalebroad = g->scalebroad;
     S.omega_max = g->omega_max;
     S.onlyharmonic = g->onlyharmonic ? 1 : 0;
@@ -264,6 +268,10 @@ int fp4_setup_system(fp4_ctx* c, const fp4_globals* g, const double* energy, con
         S.eigf = nullptr;
     }
     if ((r = c->b_list.upload(c, l0.data(), nlist * sizeof(int)))) return r;
+    std::vector<int> qc(nptk);
+    for (int q = 0; q < nptk; q++) qc[q] = ijk[3 * q] | (ijk[3 * q + 1] << 8) | (ijk[3 * q + 2] << 16);
+    if ((r = c->b_qc.upload(c, qc.data(), nptk * sizeof(int)))) return r;
+    S.qc = c->b_qc.as<int>();
     S.wv = c->b_wv.as<double4>();
     S.list0 = c->b_list.as<int>();
     // root tables exp(2 pi i x / N_d)
@@ -762,7 +770,12 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
     const int nblocks = k4_blocks(c, nwork);
-    const int subcap = 2048;
+    // per-(i,j) queue capacity: the kernel flushes when a queue could exceed it within the
+    // next capacity check (8 passes of one survivor per thread), so it must exceed 8*threads
+    const size_t bins = (size_t)nblocks * S.nb * S.nb;
+    const int min_cap = 16 * k4_threads();
+    int subcap = 4 * min_cap;
+    while (subcap > min_cap && bins * subcap * sizeof(unsigned long long) > ((size_t)4 << 30)) subcap /= 2;
     if ((r = c->b_queue.reserve(c, (size_t)nblocks * S.nb * S.nb * subcap * sizeof(unsigned long long)))) return r;
     if ((r = c->b_part.reserve(c, (size_t)nwork * nT * S.nb * 2 * sizeof(double)))) return r;
     if ((r = c->b_work.reserve(c, 64))) return r;

@@ -49,7 +49,7 @@ struct fp4_ctx {
     fp4::DevSys S{};
     std::vector<double> atom_mass;
     bool eig_packed = false;
-    DevBuffer b_energy, b_velocity, b_wv, b_eigraw, b_eig, b_eigf, b_list, b_root[3], b_rootf[3];
+    DevBuffer b_energy, b_velocity, b_wv, b_eigraw, b_eig, b_eigf, b_list, b_qc, b_root[3], b_rootf[3];
     DevBuffer b_temps, b_bose, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
     DevBuffer b_queue, b_part, b_work, b_err, b_stats;
     DevBuffer b_bte[12];
@@ -58,7 +58,7 @@ struct fp4_ctx {
     int64_t last_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double last_ms = 0.0, last_kernel_ms = 0.0;
     std::vector<DevBuffer*> all_buffers() {
-        std::vector<DevBuffer*> v = {&b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,
+        std::vector<DevBuffer*> v = {&b_qc, &b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,
                                      &b_temps,  &b_bose,     &b_out, &b_out4,   &b_lists, &b_gamma, &b_off,
                                      &b_counts, &b_queue,    &b_part, &b_work,  &b_err,   &b_stats};
         for (int d = 0; d < 3; d++) {

@@ -23,12 +23,14 @@ struct DevSys {
     int n[3];
     int nptk, nb, nlist, natoms;
     double rl[9];  // rlattvec(3,3) column-major
+    double ngd[3], rinv[3];  // ngrid(d) as double and RN(1/ngrid(d))
     double scalebroad, omega_max;
     int onlyharmonic;
     const double4* wv;
     const double2* eig;
     const float2* eigf;
     const int* list0;  // 0-based q of irreducible point ll
+    const int* qc;     // grid coordinates of q packed as a | b<<8 | c<<16 (Id2ind)
     const double2* root[3];
     const float2* rootf[3];
 };
@@ -100,6 +102,111 @@ __device__ __forceinline__ void q_coords(const DevSys& S, int q, int& a, int& b,
     c = t / S.n[1];
 }
 __device__ __forceinline__ int q_index(const DevSys& S, int a, int b, int c) { return (c * S.n[1] + b) * S.n[0] + a; }
+// table form of q_coords: one load instead of integer divisions
+__device__ __forceinline__ void q_coords_t(const DevSys& S, int q, int& a, int& b, int& c) {
+    int v = __ldg(S.qc + q);
+    a = v & 0xff;
+    b = (v >> 8) & 0xff;
+    c = v >> 16;
+}
+// (t mod N) for t in (-2N, 3N), without a division
+__device__ __forceinline__ int wrapN(int t, int N) {
+    t = (t >= N) ? t - N : t;
+    t = (t >= N) ? t - N : t;
+    t = (t < 0) ? t + N : t;
+    t = (t < 0) ? t + N : t;
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// block-wide helpers
+// ---------------------------------------------------------------------------
+// exclusive prefix of a per-thread flag, in thread order; total in `total`
+__device__ __forceinline__ int block_exclusive_scan_flag(bool flag, int* warp_tot, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+    unsigned bal = __ballot_sync(0xffffffffu, flag);
+    int pre = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < nwarp ? warp_tot[lane] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nwarp) warp_tot[lane] = incl - v;
+        if (lane == 31) warp_tot[32] = incl;
+    }
+    __syncthreads();
+    int r = warp_tot[warp] + pre;
+    total = warp_tot[32];
+    __syncthreads();
+    return r;
+}
+
+// fixed-order block sum; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < nwarp; w++) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+// fixed-order block sum of NV values at once; results valid in thread 0 (red holds 32*NV)
+template <int NV>
+__device__ __forceinline__ void block_sum_vec(double (&v)[NV], double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int x = 0; x < NV; x++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[x] += __shfl_down_sync(0xffffffffu, v[x], o);
+        if (lane == 0) red[x * 32 + warp] = v[x];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int x = 0; x < NV; x++) {
+            double t = 0.0;
+            for (int w = 0; w < nwarp; w++) t += red[x * 32 + w];
+            v[x] = t;
+        }
+    }
+    __syncthreads();
+}
+
+// Neumaier two-sum accumulation
+struct Comp {
+    double s, c;
+    __device__ __forceinline__ void add(double x) {
+        double t = s + x;
+        if (fabs(s) >= fabs(x))
+            c += (s - t) + x;
+        else
+            c += (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double val() const { return s + c; }
+};
+
+__device__ __forceinline__ int lower_bound_d(const double* a, int n, double x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
 
 // ---------------------------------------------------------------------------
 // Energy-conservation filter, bit-exact with the reference's source order.
@@ -108,6 +215,20 @@ __device__ __forceinline__ int q_index(const DevSys& S, int a, int b, int c) { r
 // then sqrt(x/2) and the scalebroad factor.  Every product and sum is
 // rounded separately (no fused multiply-add), exactly as written.
 // ---------------------------------------------------------------------------
+// x/N for a grid size N (a small positive integer), correctly rounded.
+// Reciprocal multiplication followed by two residual corrections
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34 (1990)): with r = RN(1/N) the
+// residual e = x - q*N is exact in one fused multiply-add, and q + e*r rounds
+// to RN(x/N).  tests/cuda/div_check.cu compares it with __ddiv_rn.
+__device__ __forceinline__ double div_by_grid(double x, double N, double r) {
+    double q = __dmul_rn(x, r);
+    double e = __fma_rn(-q, N, x);
+    q = __fma_rn(e, r, q);
+    e = __fma_rn(-q, N, x);
+    return __fma_rn(e, r, q);
+}
+
 __device__ __forceinline__ double sigma_exact(const DevSys& S, double4 a, double4 b) {
     double v0 = __dadd_rn(a.x, -b.x);
     double v1 = __dadd_rn(a.y, -b.y);
@@ -117,7 +238,7 @@ __device__ __forceinline__ double sigma_exact(const DevSys& S, double4 a, double
     for (int nu = 0; nu < 3; nu++) {
         const double* r = S.rl + 3 * nu;
         double dp = __dadd_rn(__dadd_rn(__dmul_rn(r[0], v0), __dmul_rn(r[1], v1)), __dmul_rn(r[2], v2));
-        double x = __ddiv_rn(dp, (double)S.n[nu]);
+        double x = div_by_grid(dp, S.ngd[nu], S.rinv[nu]);
         double x2 = __dmul_rn(x, x);
         m = (nu == 0 || x2 > m) ? x2 : m;
     }

@@ -63,6 +63,7 @@ cudaError_t launch_k3(int mode, const P3Params& p, int nmodes, cudaStream_t st);
 size_t k3_smem(int mode, const DevIfc& F, bool onlyharmonic);
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st);
 size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F);
+int k4_threads();
 cudaError_t launch_k4_reduce(const P4Params& p, double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp,
                              double* wp_pm, double* wp_mm, double rate_scale, cudaStream_t st);
 cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st);

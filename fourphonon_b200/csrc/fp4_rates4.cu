@@ -1,0 +1,576 @@
+// Four-phonon scattering-rate kernel for sm_100a.
+//
+// Persistent CTAs pull work items (q = List(ll), q', channel) from an atomic
+// counter.  For each work item:
+//   * the valid sums s_ij = w_i +- w'_j are rank-sorted in shared memory;
+//   * phase A walks every (q'', k, l) once: q''' from integer grid
+//     arithmetic, the channel's restrictions, sigma(v''-v''') in base_sigma's
+//     exact operation order (computed once for all (i,j)), a binary search for
+//     the window of s_ij that can pass the 1-sigma test, and the exact test in
+//     the reference's operation order.  Survivors are queued per (i,j);
+//   * phase B builds, per branch i, the reciprocal cluster table
+//         Z_p^{(ij)}[s][r] = sum_{c in p} kappa_c sum_{u,t} Psi_c[u][t][s][r] e_i[u] e~'_j[t]
+//     and contracts each queued process as
+//         V = sum_p w_p(q'') e~''_k[s] Z_p[s][r] conj(e'''_l[r]),
+//     with w_p(q'') = exp(+-2 pi i n''.D_p/N) read from per-class phase tables
+//     in shared memory.  This is Vp_pp/Vp_pm/Vp_mm (processes.f90:142-330)
+//     with the cluster phases factored through integer lattice coordinates.
+//   * weights (Bose factors, Gaussian, sigma floor) are FP64 for every
+//     temperature of the call; |V|^2 is formed once for all of them.
+// Per-(work item, branch, temperature) partial sums are reduced afterwards in
+// a fixed order with compensated summation (k4_reduce).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fp4_device.cuh"
+#include "fp4_internal.h"
+
+namespace fp4 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity checks
+
+template <bool MIXED>
+struct CT;
+template <>
+struct CT<false> {
+    using T = double2;
+    __device__ static T zero() { return make_double2(0.0, 0.0); }
+    __device__ static T conj(T a) { return cconj(a); }
+    __device__ static T mul(T a, T b) { return cmul(a, b); }
+    __device__ static T mac(T acc, T a, T b) { return cmac(acc, a, b); }
+    __device__ static T from(double2 a) { return a; }
+    __device__ static double norm(T a) { return a.x * a.x + a.y * a.y; }
+};
+template <>
+struct CT<true> {
+    using T = float2;
+    __device__ static T zero() { return make_float2(0.f, 0.f); }
+    __device__ static T conj(T a) { return cconjf(a); }
+    __device__ static T mul(T a, T b) { return cmulf(a, b); }
+    __device__ static T mac(T acc, T a, T b) { return cmacf(acc, a, b); }
+    __device__ static T from(double2 a) { return make_float2((float)a.x, (float)a.y); }
+    __device__ static double norm(T a) { return (double)a.x * (double)a.x + (double)a.y * (double)a.y; }
+};
+
+struct Layout {
+    size_t z, kap, pt, sval, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, misc, total;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum) {
+    Layout L;
+    const size_t cs = mixed ? 8 : 16;  // complex size
+    const size_t nb2 = (size_t)nb * nb;
+    size_t o = 0;
+    L.z = o;
+    o = al16(o + ((kind == 2) ? (size_t)nb * npi * 9 * cs : 0));
+    L.kap = o;
+    o = al16(o + ((kind == 2) ? (size_t)ntri * 16 : 0));
+    L.pt = o;
+    o = al16(o + ((kind == 2) ? (size_t)npi * lsum * cs : 0));
+    L.sval = o;
+    o = al16(o + nb2 * 8);
+    L.racc = o;
+    o = al16(o + (size_t)nb * NT * 8);
+    L.wacc = o;
+    o = al16(o + (size_t)nb * NT * 8);
+    L.pacc = o;
+    o = al16(o + (size_t)nb * 8);
+    L.red = o;
+    o = al16(o + 32 * 2 * NT * 8);
+    L.sidx = o;
+    o = al16(o + nb2 * 4);
+    L.cnt = o;
+    o = al16(o + nb2 * 4);
+    L.ncnt = o;
+    o = al16(o + (size_t)nb * 4);
+    L.klt = o;
+    o = al16(o + nb2 * 4);
+    L.pre = o;
+    o = al16(o + (size_t)(kMaxNb + 1) * 4);
+    L.misc = o;
+    o = al16(o + 8 * 4);
+    L.total = o;
+    return L;
+}
+
+template <bool MIXED>
+__device__ __forceinline__ const typename CT<MIXED>::T* eig_table(const DevSys& S);
+template <>
+__device__ __forceinline__ const double2* eig_table<false>(const DevSys& S) {
+    return S.eig;
+}
+template <>
+__device__ __forceinline__ const float2* eig_table<true>(const DevSys& S) {
+    return S.eigf;
+}
+
+// Phase B: contract every queued process of the current work item, branch by branch.
+template <int NT, bool MIXED>
+__device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout& L, const unsigned long long* qbase,
+                           int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
+                           unsigned long long& my_contr) {
+    using C = CT<MIXED>;
+    using cx = typename C::T;
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const int nb = S.nb, nb2 = nb * nb, npi = F.npi, nptk = S.nptk;
+    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2], lsum = N0 + N1 + N2;
+    cx* Z = reinterpret_cast<cx*>(smem + L.z);
+    const double2* kap = reinterpret_cast<const double2*>(smem + L.kap);
+    const cx* PT = reinterpret_cast<const cx*>(smem + L.pt);
+    double* racc = reinterpret_cast<double*>(smem + L.racc);
+    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
+    double* red = reinterpret_cast<double*>(smem + L.red);
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* pre = reinterpret_cast<int*>(smem + L.pre);
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const double floor_sigma = (double)0.001f;
+    const bool neg = (ch != 0);  // class displacement D = m_k - m_l (++) or m_l - m_k (+-, --)
+    const cx* etab = eig_table<MIXED>(S);
+    for (int i = 0; i < nb; i++) {
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int j = 0; j < nb; j++) {
+                pre[j] = acc;
+                acc += cnt[i * nb + j];
+            }
+            pre[nb] = acc;
+        }
+        __syncthreads();
+        const int tot = pre[nb];
+        if (tot == 0) {
+            __syncthreads();
+            continue;
+        }
+        if (threadIdx.x == 0) atomicAdd(&p.stats[4], 1ull);
+        // reciprocal cluster table of branch i for every j
+        const double2* ei = S.eig + (size_t)(q0 * nb + i) * nb;
+        for (int idx = threadIdx.x; idx < nb * npi * 9; idx += blockDim.x) {
+            const int j = idx / (npi * 9), rem = idx - j * (npi * 9), pc = rem / 9, sr = rem - pc * 9;
+            const double2* ej = S.eig + (size_t)(ii * nb + j) * nb;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int x = F.cl_start[pc]; x < F.cl_start[pc + 1]; x++) {
+                const int c = F.cl_index[x];
+                const int4 at = F.atoms[c];
+                const double* ph = F.phi + (size_t)c * 81 + sr;
+                double2 t1 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < 3; u++) {
+                    const double2 eu = ei[3 * at.x + u];
+#pragma unroll
+                    for (int t = 0; t < 3; t++) {
+                        double2 et = ej[3 * at.y + t];
+                        if (ch == 2) et = cconj(et);
+                        const double2 pr = cmul(eu, et);
+                        const double f = ph[(u * 3 + t) * 9];
+                        t1.x = fma(f, pr.x, t1.x);
+                        t1.y = fma(f, pr.y, t1.y);
+                    }
+                }
+                acc = cmac(acc, kap[c], t1);
+            }
+            Z[idx] = C::from(acc);
+        }
+        __syncthreads();
+        Comp accr[NT], accw[NT];
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            accr[t] = {0.0, 0.0};
+            accw[t] = {0.0, 0.0};
+        }
+        const double omega = S.wv[q0 * nb + i].w;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            int j = 0;
+            while (j + 1 < nb && pre[j + 1] <= e) j++;
+            const unsigned long long ent = qbase[(size_t)(i * nb + j) * p.subcap + (e - pre[j])];
+            const int jj = (int)(ent >> 32), k = (int)((ent >> 8) & 0xff), l = (int)(ent & 0xff);
+            int a, b, c;
+            q_coords_t(S, jj, a, b, c);
+            int t0, t1, t2;
+            if (ch == 0) {
+                t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+            } else if (ch == 1) {
+                t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+            } else {
+                t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+            }
+            const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
+            const double4 w1 = S.wv[ii * nb + j];
+            const double4 w2 = S.wv[jj * nb + k];
+            const double4 w3 = S.wv[ss * nb + l];
+            double sigma = sigma_exact(S, w2, w3);
+            const double s = (ch == 2) ? __dadd_rn(omega, -w1.w) : __dadd_rn(omega, w1.w);
+            const double delta =
+                (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w) : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
+            if (sigma <= floor_sigma) sigma = 1.0 / sqrtpi;
+            const double g = exp(-(delta * delta) / (sigma * sigma));
+            const double base = g / sigma / sqrtpi / (omega * w1.w * w2.w * w3.w);
+            double v2 = 0.0;
+            if (!S.onlyharmonic) {
+                const cx* Zj = Z + (size_t)j * npi * 9;
+                const cx* e2 = etab + (size_t)(jj * nb + k) * nb;
+                const cx* e3 = etab + (size_t)(ss * nb + l) * nb;
+                cx V = C::zero();
+                for (int blk = 0; blk < F.nblk; blk++) {
+                    const int p0 = F.blk_start[blk], p1 = F.blk_start[blk + 1];
+                    if (p0 == p1) continue;
+                    const int a3 = blk / S.natoms, a4 = blk - a3 * S.natoms;
+                    cx u[3], v[3];
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        u[x] = e2[3 * a3 + x];
+                        if (ch != 0) u[x] = C::conj(u[x]);
+                        v[x] = C::conj(e3[3 * a4 + x]);
+                    }
+                    for (int pc = p0; pc < p1; pc++) {
+                        const cx* pt = PT + pc * lsum;
+                        cx w = C::mul(C::mul(pt[a], pt[N0 + b]), pt[N0 + N1 + c]);
+                        if (neg) w = C::conj(w);
+                        const cx* z = Zj + pc * 9;
+                        cx tt = C::zero();
+#pragma unroll
+                        for (int x = 0; x < 3; x++) {
+                            cx h = C::zero();
+#pragma unroll
+                            for (int r = 0; r < 3; r++) h = C::mac(h, z[x * 3 + r], v[r]);
+                            tt = C::mac(tt, u[x], h);
+                        }
+                        V = C::mac(V, w, tt);
+                    }
+                }
+                v2 = C::norm(V);
+            }
+            my_contr++;
+            const size_t plane = (size_t)nptk * nb;
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                if (t < p.nT) {
+                    const double* bz = p.bose + t * plane;
+                    const double f1 = bz[ii * nb + j], f2 = bz[jj * nb + k], f3 = bz[ss * nb + l];
+                    double bc;
+                    if (ch == 0)
+                        bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
+                    else if (ch == 1)
+                        bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
+                    else
+                        bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
+                    const double wp4 = bc * base;
+                    accr[t].add(wp4 * v2);
+                    accw[t].add(wp4);
+                }
+            }
+        }
+        double v[2 * NT];
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            v[t] = accr[t].val();
+            v[NT + t] = accw[t].val();
+        }
+        block_sum_vec<2 * NT>(v, red);
+        if (threadIdx.x == 0) {
+            for (int t = 0; t < p.nT; t++) {
+                racc[i * NT + t] += v[t];
+                wacc[i * NT + t] += v[NT + t];
+            }
+        }
+        __syncthreads();
+    }
+    for (int x = threadIdx.x; x < nb2; x += blockDim.x) cnt[x] = 0;
+    __syncthreads();
+}
+
+template <int KIND, int NT, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
+    using C = CT<MIXED>;
+    using cx = typename C::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const int nb = S.nb, nptk = S.nptk, nb2 = nb * nb, npi = F.npi;
+    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2], lsum = N0 + N1 + N2;
+    const Layout L = k4_layout(KIND, NT, MIXED, nb, npi, F.ntri, lsum);
+    double2* kap = reinterpret_cast<double2*>(smem + L.kap);
+    cx* PT = reinterpret_cast<cx*>(smem + L.pt);
+    double* sval = reinterpret_cast<double*>(smem + L.sval);
+    double* racc = reinterpret_cast<double*>(smem + L.racc);
+    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
+    double* pacc = reinterpret_cast<double*>(smem + L.pacc);
+    double* red = reinterpret_cast<double*>(smem + L.red);
+    int* sidx = reinterpret_cast<int*>(smem + L.sidx);
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* ncnt = reinterpret_cast<int*>(smem + L.ncnt);
+    int* klt = reinterpret_cast<int*>(smem + L.klt);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+
+    // once per CTA: (k,l) decode table and per-class phase tables
+    for (int x = threadIdx.x; x < nb2; x += blockDim.x) klt[x] = ((x / nb) << 8) | (x % nb);
+    if (KIND == 2) {
+        for (int x = threadIdx.x; x < npi * lsum; x += blockDim.x) {
+            int pc = x / lsum, r = x % lsum;
+            int d = (r < N0) ? 0 : (r < N0 + N1 ? 1 : 2);
+            int xi = r - (d == 0 ? 0 : (d == 1 ? N0 : N0 + N1));
+            int4 D = F.pi_d[pc];
+            int Dd = (d == 0) ? D.x : (d == 1 ? D.y : D.z);
+            PT[x] = C::from(S.root[d][pmod(xi * Dd, S.n[d])]);
+        }
+    }
+    __syncthreads();
+
+    unsigned long long* qbase = p.queue + (size_t)blockIdx.x * nb2 * p.subcap;
+    unsigned long long my_surv = 0, my_contr = 0, my_sig = 0, my_cand = 0;
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const double floor_sigma = (double)0.001f;
+
+    for (;;) {
+        if (threadIdx.x == 0) misc[0] = atomicAdd(p.work_counter, 1);
+        __syncthreads();
+        const int wi = misc[0];
+        if (wi >= p.nwork) break;
+        const int ch = wi % 3;
+        const int rest = wi / 3;
+        const int ii = rest % nptk, ll = rest / nptk;
+        const int q0 = S.list0[ll];
+        int n0, n1, n2, m0, m1, m2;
+        q_coords_t(S, q0, n0, n1, n2);
+        q_coords_t(S, ii, m0, m1, m2);
+        // sorted branch sums s_ij = w_i +- w'_j over the valid pairs
+        for (int idx = threadIdx.x; idx < nb2; idx += blockDim.x) {
+            int i = idx / nb, j = idx % nb;
+            double wi_ = S.wv[q0 * nb + i].w, wj_ = S.wv[ii * nb + j].w;
+            bool ok = (wi_ != 0.0) && (wi_ <= S.omega_max) && (wj_ != 0.0);
+            double s = (ch == 2) ? __dadd_rn(wi_, -wj_) : __dadd_rn(wi_, wj_);
+            int rank = 0, nvalid = 0;
+            for (int y = 0; y < nb2; y++) {
+                int iy = y / nb, jy = y % nb;
+                double wiy = S.wv[q0 * nb + iy].w, wjy = S.wv[ii * nb + jy].w;
+                bool oky = (wiy != 0.0) && (wiy <= S.omega_max) && (wjy != 0.0);
+                if (!oky) continue;
+                nvalid++;
+                double sy = (ch == 2) ? __dadd_rn(wiy, -wjy) : __dadd_rn(wiy, wjy);
+                if (sy < s || (sy == s && y < idx)) rank++;
+            }
+            if (ok) {
+                sval[rank] = s;
+                sidx[rank] = idx;
+            }
+            if (idx == 0) misc[1] = nvalid;
+            cnt[idx] = 0;
+        }
+        for (int x = threadIdx.x; x < nb; x += blockDim.x) {
+            ncnt[x] = 0;
+            pacc[x] = 0.0;
+        }
+        for (int x = threadIdx.x; x < nb * NT; x += blockDim.x) {
+            racc[x] = 0.0;
+            wacc[x] = 0.0;
+        }
+        if (KIND == 2) {
+            // kappa_c = mu_c exp(2 pi i (-n.m_l +- n'.(m_j - m_l))/N)
+            for (int c = threadIdx.x; c < F.ntri; c += blockDim.x) {
+                int4 mj = F.mj[c], ml = F.ml[c];
+                double2 a = lattice_phase(S, n0, n1, n2, -ml.x, -ml.y, -ml.z);
+                int sj = (ch == 2) ? -1 : 1;
+                double2 b = lattice_phase(S, m0, m1, m2, sj * (mj.x - ml.x), sj * (mj.y - ml.y), sj * (mj.z - ml.z));
+                double2 k = cmul(a, b);
+                k.x *= F.mu[c];
+                k.y *= F.mu[c];
+                kap[c] = k;
+            }
+        }
+        __syncthreads();
+        const int ns = misc[1];
+        if (ns > 0) {
+            double smax = 0.0;
+            for (int x = 0; x < ns; x++) smax = fmax(smax, fabs(sval[x]));
+            const int jj_lo = (ch == 1) ? 0 : ii;
+            const int total = (nptk - jj_lo) * nb2;
+            // thread t covers index base+t; keep (jj, kl) of it incrementally
+            const int Bq = blockDim.x / nb2, Br = blockDim.x % nb2;
+            int cj = threadIdx.x / nb2, ckl = threadIdx.x % nb2;
+            int iter = 0;
+            for (int base = 0; base < total; base += blockDim.x, iter++) {
+                if (KIND == 2 && (iter % kCheckEvery) == 0) {
+                    if (threadIdx.x == 0) {
+                        int mx = 0;
+                        for (int b = 0; b < nb2; b++) mx = max(mx, cnt[b]);
+                        misc[2] = (mx > p.subcap - kCheckEvery * (int)blockDim.x);
+                    }
+                    __syncthreads();
+                    if (misc[2]) k4_phase_b<NT, MIXED>(p, smem, L, qbase, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+                }
+                if (base + (int)threadIdx.x < total) {
+                    const int jj = jj_lo + cj;
+                    const int kl = klt[ckl];
+                    const int k = kl >> 8, l = kl & 0xff;
+                    int a, b, c;
+                    q_coords_t(S, jj, a, b, c);
+                    int t0, t1, t2;
+                    if (ch == 0) {
+                        t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+                    } else if (ch == 1) {
+                        t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+                    } else {
+                        t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+                    }
+                    const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
+                    bool go = true;
+                    if (ch != 0 && ss < jj) go = false;
+                    if (ch != 0 && ss == jj && l < k) go = false;
+                    if (go) {
+                        const double4 w2 = S.wv[jj * nb + k];
+                        const double4 w3 = S.wv[ss * nb + l];
+                        if (w2.w != 0.0 && w3.w != 0.0) {
+                            const double sigma = sigma_exact(S, w2, w3);
+                            my_sig++;
+                            const double cen = (ch == 0) ? (w3.w - w2.w) : (w2.w + w3.w);
+                            const double tol = 1e-12 * (1.0 + fabs(w2.w) + fabs(w3.w) + smax + sigma);
+                            int x = lower_bound_d(sval, ns, cen - sigma - tol);
+                            for (; x < ns && sval[x] <= cen + sigma + tol; x++) {
+                                my_cand++;
+                                const double s = sval[x];
+                                const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w)
+                                                               : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
+                                if (!(fabs(delta) <= sigma)) continue;
+                                const int idx = sidx[x];
+                                const int i = idx / nb, j = idx - i * nb;
+                                if (ch != 1 && jj == ii && k < j) continue;
+                                if (ch == 1 && !((q0 != jj || i != k) && (q0 != ss || i != l) && (ii != jj || j != k) &&
+                                                 (ii != ss || j != l)))
+                                    continue;
+                                my_surv++;
+                                if (KIND == 0) {
+                                    atomicAdd(&ncnt[i], 1);
+                                    const double sg = (sigma <= floor_sigma) ? 1.0 / sqrtpi : sigma;
+                                    const double pc = exp(-(delta * delta) / (sg * sg)) /
+                                                      (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
+                                                       (double)(nb * nb * nb * nb));
+                                    atomicAdd(&pacc[i], pc);
+                                    continue;
+                                }
+                                const double w1 = S.wv[ii * nb + j].w;
+                                if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
+                                const int pos = atomicAdd(&cnt[idx], 1);
+                                qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
+                            }
+                        }
+                    }
+                }
+                ckl += Br;
+                cj += Bq;
+                if (ckl >= nb2) {
+                    ckl -= nb2;
+                    cj += 1;
+                }
+            }
+            if (KIND == 2) {
+                __syncthreads();
+                k4_phase_b<NT, MIXED>(p, smem, L, qbase, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+            }
+        }
+        __syncthreads();
+        if (KIND == 0) {
+            for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+                if (ncnt[i]) atomicAdd(&p.n_count[ch * S.nlist * nb + ll * nb + i], (unsigned long long)ncnt[i]);
+                if (pacc[i] != 0.0) atomicAdd(&p.p_sum[ch * S.nlist * nb + ll * nb + i], pacc[i]);
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < nb * NT; idx += blockDim.x) {
+                int i = idx / NT, t = idx % NT;
+                if (t < p.nT) {
+                    p.part_rate[((size_t)wi * p.nT + t) * nb + i] = racc[idx];
+                    p.part_wp[((size_t)wi * p.nT + t) * nb + i] = wacc[idx];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    double st[4] = {(double)my_surv, (double)my_contr, (double)my_sig, (double)my_cand};
+    block_sum_vec<4>(st, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&p.stats[0], (unsigned long long)st[0]);
+        atomicAdd(&p.stats[1], (unsigned long long)st[1]);
+        atomicAdd(&p.stats[2], (unsigned long long)st[2]);
+        atomicAdd(&p.stats[3], (unsigned long long)st[3]);
+    }
+}
+
+}  // namespace
+}  // namespace fp4
+
+namespace fp4 {
+namespace {
+
+// Fixed-order compensated reduction of the per-work-item partial sums.
+__global__ void k4_reduce(P4Params p, double* r0, double* r1, double* r2, double* w0, double* w1, double* w2,
+                          double rate_scale) {
+    const DevSys& S = p.S;
+    const int nb = S.nb, nptk = S.nptk, nl = S.nlist;
+    const int total = 3 * nl * nb * p.nT;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < total; x += gridDim.x * blockDim.x) {
+        int ch = x % 3;
+        int rest = x / 3;
+        int i = rest % nb;
+        rest /= nb;
+        int t = rest % p.nT;
+        int ll = rest / p.nT;
+        Comp ar = {0.0, 0.0}, aw = {0.0, 0.0};
+        for (int ii = 0; ii < nptk; ii++) {
+            size_t wi = ((size_t)ll * nptk + ii) * 3 + ch;
+            ar.add(p.part_rate[(wi * p.nT + t) * nb + i]);
+            aw.add(p.part_wp[(wi * p.nT + t) * nb + i]);
+        }
+        size_t o = ((size_t)t * nl + ll) * nb + i;
+        double* R = ch == 0 ? r0 : (ch == 1 ? r1 : r2);
+        double* W = ch == 0 ? w0 : (ch == 1 ? w1 : w2);
+        R[o] = ar.val() * rate_scale / nptk / nptk;
+        W[o] = aw.val() / nptk / nptk;
+    }
+}
+
+int round_nt(int nT) { return nT <= 1 ? 1 : (nT <= 2 ? 2 : (nT <= 4 ? 4 : 8)); }
+
+template <int KIND, int NT, bool MIXED>
+cudaError_t launch_k4_t(const P4Params& p, int nblocks, cudaStream_t st) {
+    size_t sm = k4_smem(KIND, p.nT, MIXED, p.S, p.F);
+    cudaError_t e = cudaFuncSetAttribute(k4_work<KIND, NT, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k4_work<KIND, NT, MIXED><<<nblocks, kThreads, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
+    Layout L = k4_layout(kind, round_nt(nT), mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2]);
+    return L.total;
+}
+
+int k4_threads() { return kThreads; }
+
+cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st) {
+    if (kind == 0) return launch_k4_t<0, 1, false>(p, nblocks, st);
+    const int NT = round_nt(nT);
+#define FP4_K4(NTV)                                                                                   \
+    if (NT == NTV) return mixed ? launch_k4_t<2, NTV, true>(p, nblocks, st) : launch_k4_t<2, NTV, false>(p, nblocks, st);
+    FP4_K4(1)
+    FP4_K4(2)
+    FP4_K4(4)
+    FP4_K4(8)
+#undef FP4_K4
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_k4_reduce(const P4Params& p, double* r0, double* r1, double* r2, double* w0, double* w1, double* w2,
+                             double rate_scale, cudaStream_t st) {
+    int total = 3 * p.S.nlist * p.S.nb * p.nT;
+    int threads = 128, blocks = (total + threads - 1) / threads;
+    k4_reduce<<<blocks, threads, 0, st>>>(p, r0, r1, r2, w0, w1, w2, rate_scale);
+    return cudaGetLastError();
+}
+
+}  // namespace fp4
