@@ -201,6 +201,30 @@ int fp4_last_stats(const fp4_ctx *ctx, int64_t *n_processes, int64_t *n_contract
                    double *kernel_ms, int64_t *launches);
 
 /*
+ * Allocation-free form of fp4_np_driver_4ph, for callers that cannot
+ * allocate device memory (a host whose device memory all comes from its own
+ * pool, or code embedded in a process whose allocator it must not touch).
+ * It has no counterpart in the reference.
+ *
+ * Same counts and phase spaces as fp4_np_driver_4ph, but: no context; every
+ * array argument is a DEVICE pointer (energy(nptk,nbands),
+ * velocity(nptk,nbands,3), List(nlist) in, the six per-mode outputs out);
+ * `stream` is a cudaStream_t (NULL: the default stream), synchronised before
+ * the call returns.  Scratch lives in one fixed 12 MiB device array that the
+ * library holds on every GPU it is loaded on until the process exits; it is
+ * enough for nptk*nbands*32 bytes of packed modes plus small tables (e.g. a
+ * 24^3 grid with 12 branches).  Larger systems return FP4_E_CAPACITY.  The
+ * first call on a device looks up the array's device address, so make that
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (other threads, other streams) race and must be
+ * serialised by the caller.  No cudaMalloc/cudaFree is ever called.
+ */
+int fp4_np_driver_4ph_noalloc(const fp4_globals *g, const double *energy, const double *velocity, int32_t nlist,
+                              const int32_t *list, int64_t *n_plusplus, double *pspace_plusplus, int64_t *n_plusminus,
+                              double *pspace_plusminus, int64_t *n_minusminus, double *pspace_minusminus,
+                              void *stream);
+
+/*
  * Work counters of the last four-phonon call: [0] surviving processes,
  * [1] contracted processes, [2] broadening evaluations (one per (q'',k,l)
  * candidate triple), [3] energy tests in the sorted windows, [4] reciprocal
