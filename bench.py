@@ -454,7 +454,10 @@ def run_ours(args):
         "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "temperatures_K": s.temperatures, "nmodes": s.nmodes,
                    "ntri4": s.ifc4.ntri, "displacement_classes": npi, "processes_per_step": last["nproc"],
-                   "contracted_per_step": last["ncontr"], "l2": "256 MiB buffer written between timed steps",
+                   "contracted_per_step": last["ncontr"],
+                   "work_counters": {"sigma_evals": int(cnt[2]), "window_tests": int(cnt[3]),
+                                     "table_builds": int(cnt[4])},
+                   "l2": "256 MiB buffer written between timed steps",
                    "parallelism": f"{world} rank(s), independent solves"},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,

@@ -254,6 +254,31 @@ class Context:
         d["rate_4ph"] = d["rate_plusplus"] + d["rate_plusminus"] + d["rate_minusminus"]
         return d
 
+    def ind_driver_4ph(self, s, n_pp, n_pm, n_mm, T=None):
+        """Ind_driver_4ph: the three channels' index lists and per-process Gamma,
+        rates and WP4 per mode.  Keys follow the oracle's ind4(), so the result
+        is also the `ind4` argument of iteration()."""
+        g = self.globals_of(s, T)
+        e, v, z, lst, ijk = self._arrays(s)
+        f = self._ifc(s.ifc4)
+        nm = s.nmodes
+        N = [np.ascontiguousarray(x, np.int64) for x in (n_pp, n_pm, n_mm)]
+        d = dict(n_pp=N[0], n_pm=N[1], n_mm=N[2])
+        lists = []
+        for ch, n in zip(("pp", "pm", "mm"), N):
+            tot = int(n.sum())
+            for key in ("ind2_", "ind3_", "ind4_"):
+                d[key + ch] = np.zeros(tot, np.int64)
+            d["gamma_" + ch] = np.zeros(tot)
+            lists += [d["ind2_" + ch], d["ind3_" + ch], d["ind4_" + ch], d["gamma_" + ch]]
+        names = ("rate_4ph", "rate_pp", "rate_pm", "rate_mm", "wp_pp", "wp_pm", "wp_mm")
+        for k in names:
+            d[k] = np.zeros(nm)
+        self._chk(self.lib.fp4_ind_driver_4ph(self.h, ct.byref(g), _p(e), _p(v), _p(z), s.nlist, _p(lst), _p(ijk),
+                                              *[_p(x) for x in N], s.ifc4.ntri, *[_p(x) for x in f],
+                                              *[_p(x) for x in lists], *[_p(d[k]) for k in names]))
+        return d
+
     # -- BTE -------------------------------------------------------------------------
     def iteration0(self, s, tau_zero):
         g = self.globals_of(s)
@@ -266,7 +291,11 @@ class Context:
                                           _p(np.ascontiguousarray(tau_zero, np.float64)), _p(F)))
         return F
 
-    def iteration(self, s, F, tau_zero, n_plus, n_minus, lists):
+    def iteration(self, s, F, tau_zero, n_plus, n_minus, lists, ind4=None):
+        """One sweep: iteration, or iteration_4ph when the 4-phonon lists
+        `ind4` (from ind_driver_4ph) are given."""
+        if ind4 is not None:
+            return self._iteration_4ph(s, F, tau_zero, n_plus, n_minus, lists, ind4)
         g = self.globals_of(s)
         e, v, _, _, _ = self._arrays(s)
         w = s.wedge
@@ -282,6 +311,30 @@ class Context:
             _p(lists["ind2_plus"]), _p(lists["ind3_plus"]), _p(lists["ind2_minus"]), _p(lists["ind3_minus"]), _p(e),
             _p(v), _p(lists["gamma_plus"]), _p(lists["gamma_minus"]), _p(np.ascontiguousarray(tau_zero, np.float64)),
             _p(F)))
+        return F
+
+    def _iteration_4ph(self, s, F, tau_zero, n_plus, n_minus, lists, ind4):
+        g = self.globals_of(s)
+        e, v, _, _, _ = self._arrays(s)
+        w = s.wedge
+        nsr = s.sym.nsymm_rot
+        symm = np.ascontiguousarray(np.transpose(s.sym.symmetrizers, (0, 2, 1))).ravel()
+        idq = np.ascontiguousarray(w.id_equi.T, np.int32)
+        n_plus = np.ascontiguousarray(n_plus, np.int32)
+        n_minus = np.ascontiguousarray(n_minus, np.int32)
+        N = [np.ascontiguousarray(ind4["n_" + ch], np.int64) for ch in ("pp", "pm", "mm")]
+        L = {k: np.ascontiguousarray(ind4[k], np.int64) for ch in ("pp", "pm", "mm")
+             for k in ("ind2_" + ch, "ind3_" + ch, "ind4_" + ch)}
+        G = [np.ascontiguousarray(ind4["gamma_" + ch], np.float64) for ch in ("pp", "pm", "mm")]
+        self._chk(self.lib.fp4_iteration_4ph(
+            self.h, ct.byref(g), s.nlist, _p(np.ascontiguousarray(w.nequi, np.int32)),
+            _p(np.ascontiguousarray(w.allequi, np.int32)), _p(np.ascontiguousarray(w.typeofsym, np.int32)), nsr,
+            _p(idq), _p(symm), _p(n_plus), _p(n_minus), int(n_plus.sum()), int(n_minus.sum()),
+            *[_p(x) for x in N], *[ct.c_int64(int(x.sum())) for x in N],
+            _p(lists["ind2_plus"]), _p(lists["ind3_plus"]), _p(lists["ind2_minus"]), _p(lists["ind3_minus"]),
+            *[_p(L[k + ch]) for ch in ("pp", "pm", "mm") for k in ("ind2_", "ind3_", "ind4_")],
+            _p(e), _p(v), _p(lists["gamma_plus"]), _p(lists["gamma_minus"]), *[_p(x) for x in G],
+            _p(np.ascontiguousarray(tau_zero, np.float64)), _p(F)))
         return F
 
     def symmetrize_fn(self, s, F):

@@ -431,6 +431,7 @@ int fp4_end(fp4_ctx* c) {
     for (int x = 0; x < 8; x++) c->last_counters[x] = (int64_t)st[x];
     if (flags & kErrQueue) return fp4_fail(c, FP4_E_CAPACITY, "an output list or work queue was smaller than the process count");
     if (flags & kErrTable) return fp4_fail(c, FP4_E_CAPACITY, "a device table limit was exceeded");
+    if (flags & kErrList) return fp4_fail(c, FP4_E_ARG, "a process list entry is out of range or breaks momentum conservation");
     return FP4_OK;
 }
 
@@ -653,8 +654,7 @@ extern "C" int fp4_ind_driver(fp4_ctx* c, const fp4_globals* g, const double* en
 // four-phonon drivers
 // ---------------------------------------------------------------------------
 static int k4_blocks(fp4_ctx* c, int nwork) {
-    int per_sm = 2;
-    int nbk = c->sm_count * per_sm;
+    int nbk = c->sm_count * k4_ctas_per_sm();
     return std::max(1, std::min(nbk, nwork));
 }
 
@@ -752,6 +752,26 @@ extern "C" int fp4_ind_only_driver_4ph(fp4_ctx* c, const fp4_globals* g, const d
     return fp4_end(c);
 }
 
+// Queue of the four-phonon work kernel: per CTA nb*nb bins of `subcap` entries of
+// (packed indices, sigma[, list position]).  The kernel flushes when a bin could
+// exceed subcap within the next capacity check (8 passes of one entry per thread),
+// so subcap must exceed 8*threads.
+static int k4_queue(fp4_ctx* c, int nblocks, bool with_pos, P4Params& p) {
+    const DevSys& S = c->S;
+    const size_t bins = (size_t)nblocks * S.nb * S.nb;
+    const int min_cap = 16 * k4_threads();
+    int subcap = 2 * min_cap;
+    const size_t entry = sizeof(unsigned long long) + sizeof(double) + (with_pos ? sizeof(long long) : 0);
+    while (subcap > min_cap && bins * subcap * entry > ((size_t)4 << 30)) subcap /= 2;
+    int r;
+    if ((r = c->b_queue.reserve(c, bins * subcap * entry))) return r;
+    p.queue = c->b_queue.as<unsigned long long>();
+    p.queue_sigma = reinterpret_cast<double*>(p.queue + bins * subcap);
+    p.queue_pos = with_pos ? reinterpret_cast<long long*>(p.queue_sigma + bins * subcap) : nullptr;
+    p.subcap = subcap;
+    return FP4_OK;
+}
+
 // Four-phonon RTA at nT temperatures; outputs device-resident in c->b_out4 as (nb,nlist,nT) x 6.
 int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     if (nT < 1 || nT > kMaxTemps) return fp4_fail(c, FP4_E_ARG, "nT=%d outside [1,%d]", nT, kMaxTemps);
@@ -770,26 +790,18 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
     const int nblocks = k4_blocks(c, nwork);
-    // per-(i,j) queue capacity: the kernel flushes when a queue could exceed it within the
-    // next capacity check (8 passes of one survivor per thread), so it must exceed 8*threads
-    const size_t bins = (size_t)nblocks * S.nb * S.nb;
-    const int min_cap = 16 * k4_threads();
-    int subcap = 4 * min_cap;
-    while (subcap > min_cap && bins * subcap * sizeof(unsigned long long) > ((size_t)4 << 30)) subcap /= 2;
-    if ((r = c->b_queue.reserve(c, (size_t)nblocks * S.nb * S.nb * subcap * sizeof(unsigned long long)))) return r;
+    P4Params p{};
+    if ((r = k4_queue(c, nblocks, false, p))) return r;
     if ((r = c->b_part.reserve(c, (size_t)nwork * nT * S.nb * 2 * sizeof(double)))) return r;
     if ((r = c->b_work.reserve(c, 64))) return r;
     if ((r = c->b_out4.reserve(c, (size_t)nm * nT * 6 * sizeof(double)))) return r;
     CK(cudaMemsetAsync(c->b_work.ptr, 0, 64, c->stream));
-    P4Params p{};
     p.S = S;
     p.F = c->ifc4.F;
     p.nT = nT;
     p.bose = c->b_bose.as<double>();
     p.nwork = nwork;
     p.work_counter = c->b_work.as<int>();
-    p.queue = c->b_queue.as<unsigned long long>();
-    p.subcap = subcap;
     p.part_rate = c->b_part.as<double>();
     p.part_wp = p.part_rate + (size_t)nwork * nT * S.nb;
     p.stats = c->b_stats.as<unsigned long long>();
@@ -826,6 +838,129 @@ extern "C" int fp4_rta_driver_4ph_multi_t(fp4_ctx* c, const fp4_globals* g, int3
     double* outs[6] = {rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm};
     for (int x = 0; x < 6; x++) CK(cudaMemcpyAsync(outs[x], o + x * blk, blk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return fp4_end(c);
+}
+
+// Ind_driver_4ph (processes.f90:3551-3822): the ordered index lists of the three
+// channels (the Ind_only enumeration), each process's Gamma stored at its list
+// position, and the per-mode rates and WP4 (fixed-order compensated sums).
+extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
+                                  const double* eigenvect, int32_t nlist, const int32_t* list, const int32_t* ijk,
+                                  const int64_t* n_pp, const int64_t* n_pm, const int64_t* n_mm, int32_t ntri,
+                                  const double* psi, const double* r_j, const double* r_k, const double* r_l,
+                                  const int32_t* index_i, const int32_t* index_j, const int32_t* index_k,
+                                  const int32_t* index_l, int64_t* i2pp, int64_t* i3pp, int64_t* i4pp,
+                                  double* gamma_pp, int64_t* i2pm, int64_t* i3pm, int64_t* i4pm, double* gamma_pm,
+                                  int64_t* i2mm, int64_t* i3mm, int64_t* i4mm, double* gamma_mm, double* rate_4ph,
+                                  double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp, double* wp_pm,
+                                  double* wp_mm) {
+    if (!c) return FP4_E_ARG;
+    if (!g || !n_pp || !n_pm || !n_mm || !rate_4ph || !rate_pp || !rate_pm || !rate_mm || !wp_pp || !wp_pm ||
+        !wp_mm || !eigenvect)
+        return fp4_fail(c, FP4_E_ARG, "null argument");
+    int r;
+    if ((r = fp4_begin(c)) || (r = fp4_setup_system(c, g, energy, velocity, eigenvect, nlist, list, ijk))) return r;
+    if ((r = fp4_setup_ifc(c, g, 4, ntri, psi, r_j, r_k, r_l, index_i, index_j, index_k, index_l, c->ifc4))) return r;
+    const DevSys& S = c->S;
+    const int nm = S.nb * nlist;
+    const bool mixed = (c->precision == FP4_PREC_MIXED);
+    size_t sm = k4_smem(3, 1, mixed, S, c->ifc4.F);
+    if (sm > 227 * 1024)
+        return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);
+    const int64_t* N[3] = {n_pp, n_pm, n_mm};
+    int64_t* O[3][3] = {{i2pp, i3pp, i4pp}, {i2pm, i3pm, i4pm}, {i2mm, i3mm, i4mm}};
+    double* GO[3] = {gamma_pp, gamma_pm, gamma_mm};
+    std::vector<long long> off((size_t)3 * (nm + 1), 0);
+    long long tot[3], base[4] = {0, 0, 0, 0};
+    for (int ch = 0; ch < 3; ch++) {
+        long long* o = off.data() + (size_t)ch * (nm + 1);
+        for (int m = 0; m < nm; m++) {
+            if (N[ch][m] < 0) return fp4_fail(c, FP4_E_ARG, "negative count");
+            o[m + 1] = o[m] + N[ch][m];
+        }
+        tot[ch] = o[nm];
+        if (tot[ch] && (!O[ch][0] || !O[ch][1] || !O[ch][2] || !GO[ch]))
+            return fp4_fail(c, FP4_E_ARG, "null process list output");
+        base[ch + 1] = base[ch] + tot[ch];
+    }
+    const size_t T = (size_t)base[3];
+    if ((r = c->b_lists.reserve(c, T * 3 * sizeof(long long) + 64)) || (r = c->b_gamma.reserve(c, T * sizeof(double) + 64)) ||
+        (r = c->b_off.reserve(c, off.size() * sizeof(long long))) ||
+        (r = c->b_counts.reserve(c, (size_t)3 * nm * sizeof(long long))))
+        return r;
+    long long* doff = c->b_off.as<long long>();
+    long long* dcnt = c->b_counts.as<long long>();
+    CK(cudaMemcpyAsync(doff, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    for (int ch = 0; ch < 3; ch++)
+        CK(cudaMemcpyAsync(dcnt + (size_t)ch * nm, N[ch], nm * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    long long* Lb = c->b_lists.as<long long>();
+    double* Gb = c->b_gamma.as<double>();
+    if (T) CK(cudaMemsetAsync(Gb, 0, T * sizeof(double), c->stream));
+    P4Params p{};
+    for (int ch = 0; ch < 3; ch++) {
+        long long* l2 = Lb + 3 * base[ch];
+        p.list_off[ch] = doff + (size_t)ch * (nm + 1);
+        p.list_n[ch] = dcnt + (size_t)ch * nm;
+        p.lind2[ch] = l2;
+        p.lind3[ch] = l2 + tot[ch];
+        p.lind4[ch] = l2 + 2 * tot[ch];
+        p.gamma_out[ch] = Gb + base[ch];
+        if (tot[ch] == 0) continue;
+        P4OrderParams q{};
+        q.S = S;
+        q.ch = ch;
+        q.list_off = p.list_off[ch];
+        q.counts = p.list_n[ch];
+        q.ind2 = l2;
+        q.ind3 = l2 + tot[ch];
+        q.ind4 = l2 + 2 * tot[ch];
+        q.err = c->b_err.as<int>();
+        CK(launch_k4_order(q, nm, c->stream));
+        c->launches++;
+    }
+    if ((r = c->b_temps.upload(c, &g->T, sizeof(double)))) return r;
+    if ((r = c->b_bose.reserve(c, (size_t)S.nptk * S.nb * sizeof(double)))) return r;
+    CK(launch_bose(S, c->b_temps.as<double>(), 1, c->b_bose.as<double>(), c->stream));
+    c->launches++;
+    const int nwork = 3 * S.nlist * S.nptk;
+    const int nblocks = k4_blocks(c, nwork);
+    if ((r = k4_queue(c, nblocks, true, p))) return r;
+    if ((r = c->b_part.reserve(c, (size_t)nwork * S.nb * 2 * sizeof(double)))) return r;
+    if ((r = c->b_work.reserve(c, 64))) return r;
+    if ((r = c->b_out4.reserve(c, (size_t)nm * 6 * sizeof(double)))) return r;
+    CK(cudaMemsetAsync(c->b_work.ptr, 0, 64, c->stream));
+    p.S = S;
+    p.F = c->ifc4.F;
+    p.nT = 1;
+    p.bose = c->b_bose.as<double>();
+    p.nwork = nwork;
+    p.work_counter = c->b_work.as<int>();
+    p.part_rate = c->b_part.as<double>();
+    p.part_wp = p.part_rate + (size_t)nwork * S.nb;
+    p.stats = c->b_stats.as<unsigned long long>();
+    p.err = c->b_err.as<int>();
+    const double rate_scale = hbarp() * hbarp() * kPi / 8.0 * (double)3.37617087f * 1.e9;
+    p.gamma_scale = rate_scale / S.nptk / S.nptk;
+    CK(cudaEventRecord(c->evk0, c->stream));
+    CK(launch_k4(3, 1, mixed, p, nblocks, c->stream));
+    CK(cudaEventRecord(c->evk1, c->stream));
+    c->kernel_timed = true;
+    c->launches++;
+    double* o = c->b_out4.as<double>();
+    CK(launch_k4_reduce(p, o, o + nm, o + 2 * nm, o + 3 * nm, o + 4 * nm, o + 5 * nm, rate_scale, c->stream));
+    c->launches++;
+    for (int ch = 0; ch < 3; ch++) {
+        if (tot[ch] == 0) continue;
+        for (int x = 0; x < 3; x++)
+            CK(cudaMemcpyAsync(O[ch][x], Lb + 3 * base[ch] + x * tot[ch], tot[ch] * sizeof(long long),
+                               cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(GO[ch], Gb + base[ch], tot[ch] * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    double* outs[6] = {rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm};
+    for (int x = 0; x < 6; x++)
+        CK(cudaMemcpyAsync(outs[x], o + (size_t)x * nm, nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((r = fp4_end(c))) return r;
+    for (int m = 0; m < nm; m++) rate_4ph[m] = rate_pp[m] + rate_pm[m] + rate_mm[m];
+    return FP4_OK;
 }
 
 extern "C" int fp4_rta_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,

@@ -1,6 +1,7 @@
 // Linearised-BTE sweep and thermal conductivity on the device.
 //
-// iteration (Src/iterations.f90:34-92) is an in-place Gauss-Seidel sweep:
+// iteration (Src/iterations.f90:34-92) and iteration_4ph (95-215, the same
+// sweep with the ++, +- and -- lists added) are in-place Gauss-Seidel sweeps:
 // modes are visited in the order (ll, i, kk) and each update reads F_n values
 // already overwritten earlier in the same sweep.  The device sweep keeps that
 // order exactly: one CTA walks the (ll, i, kk) steps in sequence and spreads
@@ -41,6 +42,14 @@ struct BteParams {
     const double* velocity;  // velocity(nptk,nb,3)
     const double* tau_zero;  // tau_zero(nb,nlist)
     double* F;               // F_n(nb,nptk,3)
+    // four-phonon lists of iteration_4ph (n4[0] == nullptr: three-phonon sweep)
+    const long long* n4[3];
+    const long long* off4[3];
+    const long long* i2_4[3];
+    const long long* i3_4[3];
+    const long long* i4_4[3];
+    const double* g4[3];
+    int* err;
 };
 
 __device__ __forceinline__ double& Fat(const BteParams& p, int b, int q, int d) {
@@ -57,14 +66,50 @@ __global__ void __launch_bounds__(1024) k_sweep(BteParams p) {
             const int mm = ll * nb + i;
             const int np_ = p.n_plus[mm], nm_ = p.n_minus[mm];
             const long long op = p.off_plus[mm], om = p.off_minus[mm];
+            long long c4[3] = {0, 0, 0};
+            if (p.n4[0])
+                for (int ch = 0; ch < 3; ch++) c4[ch] = p.n4[ch][mm];
+            const long long n3ph = (long long)np_ + nm_, ntot = n3ph + c4[0] + c4[1] + c4[2];
+            const long long lim = (long long)p.nptk * nb;
             for (int kk = 0; kk < p.nequi[ll]; kk++) {
                 const int qq = p.allequi[ll * p.nsr + kk] - 1;
                 const int sym = p.typeofsym[ll * p.nsr + kk] - 1;
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-                for (int x = threadIdx.x; x < np_ + nm_; x += blockDim.x) {
+                for (long long x = threadIdx.x; x < ntot; x += blockDim.x) {
+                    if (x >= n3ph) {
+                        // iteration_4ph: ++ Gamma(F_l - F_j - F_k), +- Gamma(F_l - F_j + F_k),
+                        // -- Gamma(F_l + F_j + F_k), q-points mapped by the same symmetry
+                        long long y = x - n3ph;
+                        int ch = 0;
+                        while (ch < 2 && y >= c4[ch]) {
+                            y -= c4[ch];
+                            ch++;
+                        }
+                        const long long o = p.off4[ch][mm] + y;
+                        const long long y2 = p.i2_4[ch][o] - 1, y3 = p.i3_4[ch][o] - 1, y4 = p.i4_4[ch][o] - 1;
+                        if (y2 < 0 || y2 >= lim || y3 < 0 || y3 >= lim || y4 < 0 || y4 >= lim) {
+                            atomicOr(p.err, kErrList);
+                            continue;
+                        }
+                        const int j = (int)(y2 % nb), k = (int)(y3 % nb), l = (int)(y4 % nb);
+                        const int qj = p.id_equi[(y2 / nb) * p.nsr + sym] - 1;
+                        const int qk = p.id_equi[(y3 / nb) * p.nsr + sym] - 1;
+                        const int ql = p.id_equi[(y4 / nb) * p.nsr + sym] - 1;
+                        const double g = p.g4[ch][o];
+                        const double sj = (ch == 2) ? 1.0 : -1.0, sk = (ch == 0) ? -1.0 : 1.0;
+                        // F_l -+ F_j -+ F_k with the reference's left-to-right order
+                        a0 += g * ((Fat(p, l, ql, 0) + sj * Fat(p, j, qj, 0)) + sk * Fat(p, k, qk, 0));
+                        a1 += g * ((Fat(p, l, ql, 1) + sj * Fat(p, j, qj, 1)) + sk * Fat(p, k, qk, 1));
+                        a2 += g * ((Fat(p, l, ql, 2) + sj * Fat(p, j, qj, 2)) + sk * Fat(p, k, qk, 2));
+                        continue;
+                    }
                     const bool plus = x < np_;
                     const long long o = plus ? op + x : om + (x - np_);
                     const int x2 = (plus ? p.i2p : p.i2m)[o] - 1, x3 = (plus ? p.i3p : p.i3m)[o] - 1;
+                    if (x2 < 0 || x2 >= lim || x3 < 0 || x3 >= lim) {
+                        atomicOr(p.err, kErrList);
+                        continue;
+                    }
                     const int j = x2 % nb, m2 = x2 / nb, k = x3 % nb, n3 = x3 / nb;
                     const int qa = p.id_equi[(size_t)n3 * p.nsr + sym] - 1;
                     const int qb = p.id_equi[(size_t)m2 * p.nsr + sym] - 1;
@@ -237,12 +282,24 @@ extern "C" int fp4_iteration0(fp4_ctx* c, const fp4_globals* g, int32_t nlist, c
     return fp4_end(c);
 }
 
-extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
-                             const int32_t* allequi, const int32_t* typeofsym, int32_t nsr, const int32_t* id_equi,
-                             const double* symmetrizers, const int32_t* n_plus, const int32_t* n_minus,
-                             int32_t ntotal_plus, int32_t ntotal_minus, const int32_t* i2p, const int32_t* i3p,
-                             const int32_t* i2m, const int32_t* i3m, const double* omega, const double* velocity,
-                             const double* gp, const double* gm, const double* tau_zero, double* f_n) {
+namespace {
+// The four-phonon arguments of iteration_4ph (all null for the three-phonon sweep).
+struct Lists4 {
+    const int64_t* n[3];
+    int64_t ntotal[3];
+    const int64_t* i2[3];
+    const int64_t* i3[3];
+    const int64_t* i4[3];
+    const double* g[3];
+};
+}  // namespace
+
+static int run_sweep(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi, const int32_t* allequi,
+                     const int32_t* typeofsym, int32_t nsr, const int32_t* id_equi, const double* symmetrizers,
+                     const int32_t* n_plus, const int32_t* n_minus, int32_t ntotal_plus, int32_t ntotal_minus,
+                     const int32_t* i2p, const int32_t* i3p, const int32_t* i2m, const int32_t* i3m,
+                     const double* omega, const double* velocity, const double* gp, const double* gm,
+                     const double* tau_zero, double* f_n, const Lists4* l4) {
     if (!c) return FP4_E_ARG;
     int r;
     if ((r = check_g(c, g))) return r;
@@ -254,6 +311,7 @@ extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, co
     const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2], nm = nb * nlist;
     std::vector<long long> op(nm + 1, 0), om(nm + 1, 0);
     for (int m = 0; m < nm; m++) {
+        if (n_plus[m] < 0 || n_minus[m] < 0) return fp4_fail(c, FP4_E_ARG, "negative count");
         op[m + 1] = op[m] + n_plus[m];
         om[m + 1] = om[m] + n_minus[m];
     }
@@ -261,6 +319,30 @@ extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, co
         return fp4_fail(c, FP4_E_ARG, "sum(N_plus)/sum(N_minus) differ from Ntotal_plus/Ntotal_minus");
     for (int q = 0; q < nptk * nsr; q++)
         if (id_equi[q] < 1 || id_equi[q] > nptk) return fp4_fail(c, FP4_E_ARG, "ID_equi entry outside [1,nptk]");
+    for (int ll = 0; ll < nlist; ll++) {
+        if (nequi[ll] < 0 || nequi[ll] > nsr) return fp4_fail(c, FP4_E_ARG, "Nequi entry outside [0,nsymm_rot]");
+        for (int kk = 0; kk < nequi[ll]; kk++) {
+            const int q = ll * nsr + kk;
+            if (typeofsym[q] < 1 || typeofsym[q] > nsr || allequi[q] < 1 || allequi[q] > nptk)
+                return fp4_fail(c, FP4_E_ARG, "TypeofSymmetry/ALLEquiList entry out of range");
+        }
+    }
+    std::vector<long long> off4;
+    if (l4) {
+        off4.assign((size_t)3 * (nm + 1), 0);
+        for (int ch = 0; ch < 3; ch++) {
+            if (!l4->n[ch]) return fp4_fail(c, FP4_E_ARG, "null 4-phonon counts");
+            long long* o = off4.data() + (size_t)ch * (nm + 1);
+            for (int m = 0; m < nm; m++) {
+                if (l4->n[ch][m] < 0) return fp4_fail(c, FP4_E_ARG, "negative count");
+                o[m + 1] = o[m] + l4->n[ch][m];
+            }
+            if (o[nm] != l4->ntotal[ch])
+                return fp4_fail(c, FP4_E_ARG, "sum(N_plusplus/plusminus/minusminus) differs from its Ntotal");
+            if (o[nm] && (!l4->i2[ch] || !l4->i3[ch] || !l4->i4[ch] || !l4->g[ch]))
+                return fp4_fail(c, FP4_E_ARG, "null 4-phonon process list");
+        }
+    }
     if ((r = fp4_begin(c))) return r;
     DevBuffer* B = c->b_bte;
     if ((r = B[0].upload(c, nequi, nlist * sizeof(int))) || (r = B[1].upload(c, allequi, (size_t)nlist * nsr * sizeof(int))) ||
@@ -319,12 +401,72 @@ extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, co
     p.i3m = L + 2 * tp + tm;
     p.gp = G;
     p.gm = G + tp;
+    p.err = c->b_err.as<int>();
+    if (l4) {
+        // [n4 (3 x nm) | off4 (3 x (nm+1))] and [i2|i3|i4 per channel] and [gamma per channel]
+        const size_t t4 = (size_t)(l4->ntotal[0] + l4->ntotal[1] + l4->ntotal[2]);
+        if ((r = c->b_counts.reserve(c, ((size_t)3 * nm + off4.size()) * sizeof(long long))) ||
+            (r = c->b_lists.reserve(c, t4 * 3 * sizeof(long long) + 64)) ||
+            (r = c->b_gamma.reserve(c, t4 * sizeof(double) + 64)))
+            return r;
+        long long* dn = c->b_counts.as<long long>();
+        long long* doff = dn + 3 * nm;
+        long long* L4 = c->b_lists.as<long long>();
+        double* G4 = c->b_gamma.as<double>();
+        CK(cudaMemcpyAsync(doff, off4.data(), off4.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        size_t base = 0;
+        for (int ch = 0; ch < 3; ch++) {
+            const size_t t = (size_t)l4->ntotal[ch];
+            CK(cudaMemcpyAsync(dn + (size_t)ch * nm, l4->n[ch], nm * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+            long long* l = L4 + 3 * base;
+            if (t) {
+                CK(cudaMemcpyAsync(l, l4->i2[ch], t * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+                CK(cudaMemcpyAsync(l + t, l4->i3[ch], t * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+                CK(cudaMemcpyAsync(l + 2 * t, l4->i4[ch], t * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+                CK(cudaMemcpyAsync(G4 + base, l4->g[ch], t * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            }
+            p.n4[ch] = dn + (size_t)ch * nm;
+            p.off4[ch] = doff + (size_t)ch * (nm + 1);
+            p.i2_4[ch] = l;
+            p.i3_4[ch] = l + t;
+            p.i4_4[ch] = l + 2 * t;
+            p.g4[ch] = G4 + base;
+            base += t;
+        }
+    }
     k_sweep<<<1, 1024, 0, c->stream>>>(p);
     CK(cudaGetLastError());
     c->launches++;
     CK(cudaMemcpyAsync(f_n, B[5].ptr, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     B[5].key = 0;  // device copy now differs from the caller's previous F_n
     return fp4_end(c);
+}
+
+extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
+                             const int32_t* allequi, const int32_t* typeofsym, int32_t nsr, const int32_t* id_equi,
+                             const double* symmetrizers, const int32_t* n_plus, const int32_t* n_minus,
+                             int32_t ntotal_plus, int32_t ntotal_minus, const int32_t* i2p, const int32_t* i3p,
+                             const int32_t* i2m, const int32_t* i3m, const double* omega, const double* velocity,
+                             const double* gp, const double* gm, const double* tau_zero, double* f_n) {
+    return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
+                     ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, nullptr);
+}
+
+extern "C" int fp4_iteration_4ph(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
+                                 const int32_t* allequi, const int32_t* typeofsym, int32_t nsr,
+                                 const int32_t* id_equi, const double* symmetrizers, const int32_t* n_plus,
+                                 const int32_t* n_minus, int32_t ntotal_plus, int32_t ntotal_minus,
+                                 const int64_t* n_pp, const int64_t* n_pm, const int64_t* n_mm, int64_t ntotal_pp,
+                                 int64_t ntotal_pm, int64_t ntotal_mm, const int32_t* i2p, const int32_t* i3p,
+                                 const int32_t* i2m, const int32_t* i3m, const int64_t* i2pp, const int64_t* i3pp,
+                                 const int64_t* i4pp, const int64_t* i2pm, const int64_t* i3pm, const int64_t* i4pm,
+                                 const int64_t* i2mm, const int64_t* i3mm, const int64_t* i4mm, const double* omega,
+                                 const double* velocity, const double* gp, const double* gm, const double* gpp,
+                                 const double* gpm, const double* gmm, const double* tau_zero, double* f_n) {
+    Lists4 l4{{n_pp, n_pm, n_mm}, {ntotal_pp, ntotal_pm, ntotal_mm}, {i2pp, i2pm, i2mm}, {i3pp, i3pm, i3mm},
+              {i4pp, i4pm, i4mm}, {gpp, gpm, gmm}};
+    return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
+                     ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, &l4);
 }
 
 extern "C" int fp4_symmetrize_fn(fp4_ctx* c, const fp4_globals* g, const double* symmetrizers, double* f_n) {

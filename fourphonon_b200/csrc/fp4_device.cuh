@@ -257,6 +257,6 @@ __device__ __forceinline__ unsigned long long pack4(int jj, int j, int k, int l)
 }
 
 // Error flags raised by kernels (read back by the host after each call)
-enum : int { kErrQueue = 1, kErrTable = 2 };
+enum : int { kErrQueue = 1, kErrTable = 2, kErrList = 4 };
 
 }  // namespace fp4

@@ -38,6 +38,7 @@ struct P4Params {
     int* work_counter;
     int ch_of_work[3];
     unsigned long long* queue;  // per CTA nb*nb bins of subcap entries
+    double* queue_sigma;        // broadening of each queued process, same indexing as queue
     int subcap;
     double* part_rate;  // [work][t][i]
     double* part_wp;
@@ -45,6 +46,15 @@ struct P4Params {
     double* p_sum;                // NP: [ch][mode]
     unsigned long long* stats;    // [0] surviving processes, [1] contracted
     int* err;
+    // kind 3 (Ind_driver_4ph): the ordered lists of each channel and its Gamma output
+    const long long* list_off[3];  // Naccum(mm)
+    const long long* list_n[3];    // N(mm)
+    const long long* lind2[3];
+    const long long* lind3[3];
+    const long long* lind4[3];
+    double* gamma_out[3];
+    double gamma_scale;     // hbarp^2 pi/8 * 3.37617087 * 1e9 / nptk^2
+    long long* queue_pos;   // list position of each queued process, same indexing as queue
 };
 
 struct P4OrderParams {
@@ -64,6 +74,7 @@ size_t k3_smem(int mode, const DevIfc& F, bool onlyharmonic);
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st);
 size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F);
 int k4_threads();
+int k4_ctas_per_sm();
 cudaError_t launch_k4_reduce(const P4Params& p, double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp,
                              double* wp_pm, double* wp_mm, double rate_scale, cudaStream_t st);
 cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st);

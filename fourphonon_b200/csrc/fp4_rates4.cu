@@ -31,6 +31,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity checks
+#ifndef FP4_K4_CTAS_PER_SM
+#define FP4_K4_CTAS_PER_SM 2
+#endif
+constexpr int kCtasPerSm = FP4_K4_CTAS_PER_SM;  // resident persistent CTAs per SM (register budget)
 
 template <bool MIXED>
 struct CT;
@@ -56,7 +60,7 @@ struct CT<true> {
 };
 
 struct Layout {
-    size_t z, kap, pt, sval, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, misc, total;
+    size_t z, kap, pt, sval, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, misc, total;
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -67,11 +71,11 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
     const size_t nb2 = (size_t)nb * nb;
     size_t o = 0;
     L.z = o;
-    o = al16(o + ((kind == 2) ? (size_t)nb * npi * 9 * cs : 0));
+    o = al16(o + ((kind >= 2) ? (size_t)nb * npi * 9 * cs : 0));
     L.kap = o;
-    o = al16(o + ((kind == 2) ? (size_t)ntri * 16 : 0));
+    o = al16(o + ((kind >= 2) ? (size_t)ntri * 16 : 0));
     L.pt = o;
-    o = al16(o + ((kind == 2) ? (size_t)npi * lsum * cs : 0));
+    o = al16(o + ((kind >= 2) ? (size_t)npi * lsum * cs : 0));
     L.sval = o;
     o = al16(o + nb2 * 8);
     L.racc = o;
@@ -92,6 +96,10 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
     o = al16(o + nb2 * 4);
     L.pre = o;
     o = al16(o + (size_t)(kMaxNb + 1) * 4);
+    L.blk = o;  // non-empty atom-pair blocks of the class table: (first class, end, atom k, atom l)
+    o = al16(o + (size_t)(kMaxNb / 3) * (kMaxNb / 3) * 16);
+    L.seg = o;  // kind 3: first list position of each branch's q' segment, then the segments' prefix
+    o = al16(o + (size_t)(2 * nb + 1) * 8);
     L.misc = o;
     o = al16(o + 8 * 4);
     L.total = o;
@@ -110,10 +118,11 @@ __device__ __forceinline__ const float2* eig_table<true>(const DevSys& S) {
 }
 
 // Phase B: contract every queued process of the current work item, branch by branch.
-template <int NT, bool MIXED>
+// LIST: also store each process's own Gamma at its list position (Ind_plusplus etc.).
+template <int NT, bool MIXED, bool LIST>
 __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout& L, const unsigned long long* qbase,
-                           int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
-                           unsigned long long& my_contr) {
+                           const double* qsig, const long long* qpos, int ch, int ii, int q0, int m0, int m1, int m2,
+                           int n0, int n1, int n2, unsigned long long& my_contr) {
     using C = CT<MIXED>;
     using cx = typename C::T;
     const DevSys& S = p.S;
@@ -128,6 +137,8 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
     double* red = reinterpret_cast<double*>(smem + L.red);
     int* cnt = reinterpret_cast<int*>(smem + L.cnt);
     int* pre = reinterpret_cast<int*>(smem + L.pre);
+    const int4* blkinfo = reinterpret_cast<const int4*>(smem + L.blk);
+    const int nbk = reinterpret_cast<const int*>(smem + L.misc)[3];
     const double sqrtpi = sqrt(3.141592653589793238);
     const double floor_sigma = (double)0.001f;
     const bool neg = (ch != 0);  // class displacement D = m_k - m_l (++) or m_l - m_k (+-, --)
@@ -177,17 +188,22 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
             Z[idx] = C::from(acc);
         }
         __syncthreads();
-        Comp accr[NT], accw[NT];
+        // plain per-thread partial sums (a few tens of terms each); the cross-work-item
+        // reduction (k4_reduce) is the compensated one
+        double accr[NT], accw[NT];
 #pragma unroll
         for (int t = 0; t < NT; t++) {
-            accr[t] = {0.0, 0.0};
-            accw[t] = {0.0, 0.0};
+            accr[t] = 0.0;
+            accw[t] = 0.0;
         }
-        const double omega = S.wv[q0 * nb + i].w;
+        const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;  // omega field of the (v,w) records
+        const double omega = wvw[4 * (q0 * nb + i)];
         for (int e = threadIdx.x; e < tot; e += blockDim.x) {
             int j = 0;
             while (j + 1 < nb && pre[j + 1] <= e) j++;
-            const unsigned long long ent = qbase[(size_t)(i * nb + j) * p.subcap + (e - pre[j])];
+            const size_t qi = (size_t)(i * nb + j) * p.subcap + (e - pre[j]);
+            const unsigned long long ent = qbase[qi];
+            double sigma = qsig[qi];
             const int jj = (int)(ent >> 32), k = (int)((ent >> 8) & 0xff), l = (int)(ent & 0xff);
             int a, b, c;
             q_coords_t(S, jj, a, b, c);
@@ -200,26 +216,23 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
                 t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
             }
             const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
-            const double4 w1 = S.wv[ii * nb + j];
-            const double4 w2 = S.wv[jj * nb + k];
-            const double4 w3 = S.wv[ss * nb + l];
-            double sigma = sigma_exact(S, w2, w3);
-            const double s = (ch == 2) ? __dadd_rn(omega, -w1.w) : __dadd_rn(omega, w1.w);
-            const double delta =
-                (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w) : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
+            const double w1 = wvw[4 * (ii * nb + j)];
+            const double w2 = wvw[4 * (jj * nb + k)];
+            const double w3 = wvw[4 * (ss * nb + l)];
+            const double s = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
+            const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2), -w3) : __dadd_rn(__dadd_rn(s, -w2), -w3);
             if (sigma <= floor_sigma) sigma = 1.0 / sqrtpi;
             const double g = exp(-(delta * delta) / (sigma * sigma));
-            const double base = g / sigma / sqrtpi / (omega * w1.w * w2.w * w3.w);
+            const double base = g / (sigma * sqrtpi * (omega * w1 * w2 * w3));
             double v2 = 0.0;
-            if (!S.onlyharmonic) {
+            if (LIST || !S.onlyharmonic) {
                 const cx* Zj = Z + (size_t)j * npi * 9;
                 const cx* e2 = etab + (size_t)(jj * nb + k) * nb;
                 const cx* e3 = etab + (size_t)(ss * nb + l) * nb;
                 cx V = C::zero();
-                for (int blk = 0; blk < F.nblk; blk++) {
-                    const int p0 = F.blk_start[blk], p1 = F.blk_start[blk + 1];
-                    if (p0 == p1) continue;
-                    const int a3 = blk / S.natoms, a4 = blk - a3 * S.natoms;
+                for (int bb = 0; bb < nbk; bb++) {
+                    const int4 bi = blkinfo[bb];
+                    const int p0 = bi.x, p1 = bi.y, a3 = bi.z, a4 = bi.w;
                     cx u[3], v[3];
 #pragma unroll
                     for (int x = 0; x < 3; x++) {
@@ -260,16 +273,17 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
                     else
                         bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
                     const double wp4 = bc * base;
-                    accr[t].add(wp4 * v2);
-                    accw[t].add(wp4);
+                    accr[t] = fma(wp4, v2, accr[t]);
+                    accw[t] += wp4;
+                    if (LIST) p.gamma_out[ch][qpos[qi]] = wp4 * v2 * p.gamma_scale;
                 }
             }
         }
         double v[2 * NT];
 #pragma unroll
         for (int t = 0; t < NT; t++) {
-            v[t] = accr[t].val();
-            v[NT + t] = accw[t].val();
+            v[t] = accr[t];
+            v[NT + t] = accw[t];
         }
         block_sum_vec<2 * NT>(v, red);
         if (threadIdx.x == 0) {
@@ -284,8 +298,109 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
     __syncthreads();
 }
 
+// True (for the whole CTA) when some (i,j) queue could overflow within the next
+// kCheckEvery passes of at most one new entry per thread.
+__device__ __forceinline__ bool queue_nearly_full(const P4Params& p, const int* cnt, int nb2, int* misc) {
+    if (threadIdx.x == 0) {
+        int mx = 0;
+        for (int b = 0; b < nb2; b++) mx = max(mx, cnt[b]);
+        misc[2] = (mx > p.subcap - kCheckEvery * (int)blockDim.x);
+    }
+    __syncthreads();
+    return misc[2] != 0;
+}
+
+// Ind_driver_4ph work item: instead of enumerating, read the processes of q' = ii
+// from the channel's ordered lists (one contiguous segment per branch i, found by
+// bisection: the lists are ordered by q' within each mode) and queue them with
+// their list positions; phase B then stores each Gamma in place.  Entries that are
+// out of range or break momentum conservation raise kErrList and are skipped.
+template <int NT, bool MIXED>
+__device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const Layout& L, unsigned long long* qbase,
+                                double* qsig, long long* qpos, int ch, int ii, int ll, int q0, int m0, int m1, int m2,
+                                int n0, int n1, int n2, unsigned long long& my_surv, unsigned long long& my_contr) {
+    const DevSys& S = p.S;
+    const int nb = S.nb, nb2 = nb * nb, nptk = S.nptk;
+    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2];
+    long long* seglo = reinterpret_cast<long long*>(smem + L.seg);
+    long long* segpre = seglo + nb;
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+    const long long* I2 = p.lind2[ch];
+    const long long* I3 = p.lind3[ch];
+    const long long* I4 = p.lind4[ch];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const int mm = ll * nb + i;
+        const long long o = p.list_off[ch][mm], n = p.list_n[ch][mm];
+        long long lo = o, hi = o + n;
+        while (lo < hi) {  // first entry with q' >= ii
+            const long long mid = (lo + hi) >> 1;
+            if ((I2[mid] - 1) / nb < ii) lo = mid + 1; else hi = mid;
+        }
+        const long long a = lo;
+        hi = o + n;
+        while (lo < hi) {  // first entry with q' > ii
+            const long long mid = (lo + hi) >> 1;
+            if ((I2[mid] - 1) / nb <= ii) lo = mid + 1; else hi = mid;
+        }
+        seglo[i] = a;
+        segpre[i + 1] = lo - a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        segpre[0] = 0;
+        for (int i = 0; i < nb; i++) segpre[i + 1] += segpre[i];
+    }
+    __syncthreads();
+    const long long total = segpre[nb];
+    const long long lim = (long long)nptk * nb;
+    int iter = 0;
+    for (long long base = 0; base < total; base += blockDim.x, iter++) {
+        if ((iter % kCheckEvery) == 0 && queue_nearly_full(p, cnt, nb2, misc))
+            k4_phase_b<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+        const long long e = base + threadIdx.x;
+        if (e >= total) continue;
+        int i = 0;
+        while (i + 1 < nb && segpre[i + 1] <= e) i++;
+        const long long pos = seglo[i] + (e - segpre[i]);
+        const long long x2 = I2[pos] - 1, x3 = I3[pos] - 1, x4 = I4[pos] - 1;
+        bool ok = x2 >= 0 && x2 < lim && x3 >= 0 && x3 < lim && x4 >= 0 && x4 < lim && x2 / nb == ii;
+        const int j = (int)(x2 % nb), jj = (int)(x3 / nb), k = (int)(x3 % nb), ss = (int)(x4 / nb), l = (int)(x4 % nb);
+        if (ok) {
+            int a, b, c;
+            q_coords_t(S, jj, a, b, c);
+            int t0, t1, t2;
+            if (ch == 0) {
+                t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+            } else if (ch == 1) {
+                t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+            } else {
+                t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+            }
+            ok = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2)) == ss;
+        }
+        if (!ok) {
+            atomicOr(p.err, kErrList);
+            continue;
+        }
+        my_surv++;
+        const double w1 = S.wv[ii * nb + j].w;
+        const double4 w2 = S.wv[jj * nb + k];
+        const double4 w3 = S.wv[ss * nb + l];
+        if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0, Gamma = 0 (output pre-zeroed)
+        const int idx = i * nb + j;
+        const int qp = atomicAdd(&cnt[idx], 1);
+        const size_t qi = (size_t)idx * p.subcap + qp;
+        qbase[qi] = pack4(jj, j, k, l);
+        qsig[qi] = sigma_exact(S, w2, w3);
+        qpos[qi] = pos;
+    }
+    __syncthreads();
+    k4_phase_b<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+}
+
 template <int KIND, int NT, bool MIXED>
-__global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k4_work(P4Params p) {
     using C = CT<MIXED>;
     using cx = typename C::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -307,9 +422,18 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
     int* klt = reinterpret_cast<int*>(smem + L.klt);
     int* misc = reinterpret_cast<int*>(smem + L.misc);
 
-    // once per CTA: (k,l) decode table and per-class phase tables
+    // once per CTA: (k,l) decode table, non-empty class blocks and per-class phase tables
     for (int x = threadIdx.x; x < nb2; x += blockDim.x) klt[x] = ((x / nb) << 8) | (x % nb);
-    if (KIND == 2) {
+    if (threadIdx.x == 0) {
+        int4* blkinfo = reinterpret_cast<int4*>(smem + L.blk);
+        int nbk = 0;
+        if (KIND >= 2)
+            for (int b = 0; b < F.nblk; b++)
+                if (F.blk_start[b] < F.blk_start[b + 1])
+                    blkinfo[nbk++] = make_int4(F.blk_start[b], F.blk_start[b + 1], b / S.natoms, b % S.natoms);
+        misc[3] = nbk;
+    }
+    if (KIND >= 2) {
         for (int x = threadIdx.x; x < npi * lsum; x += blockDim.x) {
             int pc = x / lsum, r = x % lsum;
             int d = (r < N0) ? 0 : (r < N0 + N1 ? 1 : 2);
@@ -322,6 +446,9 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
     __syncthreads();
 
     unsigned long long* qbase = p.queue + (size_t)blockIdx.x * nb2 * p.subcap;
+    double* qsig = p.queue_sigma + (size_t)blockIdx.x * nb2 * p.subcap;
+    long long* qpos = (KIND == 3) ? p.queue_pos + (size_t)blockIdx.x * nb2 * p.subcap : nullptr;
+    constexpr bool LIST = (KIND == 3);
     unsigned long long my_surv = 0, my_contr = 0, my_sig = 0, my_cand = 0;
     const double sqrtpi = sqrt(3.141592653589793238);
     const double floor_sigma = (double)0.001f;
@@ -369,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
             racc[x] = 0.0;
             wacc[x] = 0.0;
         }
-        if (KIND == 2) {
+        if (KIND >= 2) {
             // kappa_c = mu_c exp(2 pi i (-n.m_l +- n'.(m_j - m_l))/N)
             for (int c = threadIdx.x; c < F.ntri; c += blockDim.x) {
                 int4 mj = F.mj[c], ml = F.ml[c];
@@ -384,7 +511,10 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
         }
         __syncthreads();
         const int ns = misc[1];
-        if (ns > 0) {
+        if (KIND == 3) {
+            k4_list_segment<NT, MIXED>(p, smem, L, qbase, qsig, qpos, ch, ii, ll, q0, m0, m1, m2, n0, n1, n2, my_surv,
+                                       my_contr);
+        } else if (ns > 0) {
             double smax = 0.0;
             for (int x = 0; x < ns; x++) smax = fmax(smax, fabs(sval[x]));
             const int jj_lo = (ch == 1) ? 0 : ii;
@@ -395,13 +525,9 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
             int iter = 0;
             for (int base = 0; base < total; base += blockDim.x, iter++) {
                 if (KIND == 2 && (iter % kCheckEvery) == 0) {
-                    if (threadIdx.x == 0) {
-                        int mx = 0;
-                        for (int b = 0; b < nb2; b++) mx = max(mx, cnt[b]);
-                        misc[2] = (mx > p.subcap - kCheckEvery * (int)blockDim.x);
-                    }
-                    __syncthreads();
-                    if (misc[2]) k4_phase_b<NT, MIXED>(p, smem, L, qbase, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+                    if (queue_nearly_full(p, cnt, nb2, misc))
+                        k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                                                    my_contr);
                 }
                 if (base + (int)threadIdx.x < total) {
                     const int jj = jj_lo + cj;
@@ -456,6 +582,7 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
                                 if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
                                 const int pos = atomicAdd(&cnt[idx], 1);
                                 qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
+                                qsig[(size_t)idx * p.subcap + pos] = sigma;
                             }
                         }
                     }
@@ -469,7 +596,8 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work(P4Params p) {
             }
             if (KIND == 2) {
                 __syncthreads();
-                k4_phase_b<NT, MIXED>(p, smem, L, qbase, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+                k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                                            my_contr);
             }
         }
         __syncthreads();
@@ -551,9 +679,14 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
+int k4_ctas_per_sm() { return kCtasPerSm; }
 
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st) {
     if (kind == 0) return launch_k4_t<0, 1, false>(p, nblocks, st);
+    if (kind == 3) {
+        if (nT != 1) return cudaErrorInvalidValue;
+        return mixed ? launch_k4_t<3, 1, true>(p, nblocks, st) : launch_k4_t<3, 1, false>(p, nblocks, st);
+    }
     const int NT = round_nt(nT);
 #define FP4_K4(NTV)                                                                                   \
     if (NT == NTV) return mixed ? launch_k4_t<2, NTV, true>(p, nblocks, st) : launch_k4_t<2, NTV, false>(p, nblocks, st);

@@ -158,6 +158,25 @@ int fp4_ind_driver(fp4_ctx *ctx, const fp4_globals *g, const double *energy, con
                    double *rate_minus, double *wp3_plus, double *wp3_minus);
 
 /*
+ * Replaces Ind_driver_4ph (Src/processes.f90:3551-3822) with Ind_plusplus,
+ * Ind_plusminus and Ind_minusminus (3254-3548): the 4-phonon index lists of
+ * the three channels in the reference's order at the Naccum offsets of
+ * N_plusplus etc., each process's Gamma (hbarp^2 pi/8 WP4 |Vp|^2 in THz, no
+ * extra factor), the per-mode rates (sum of the mode's Gammas), rate_4ph and
+ * WP4 per mode.  Memory: 32 bytes per listed process on the device.
+ */
+int fp4_ind_driver_4ph(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                       const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk,
+                       const int64_t *n_plusplus, const int64_t *n_plusminus, const int64_t *n_minusminus,
+                       int32_t ntri, const double *psi, const double *r_j, const double *r_k, const double *r_l,
+                       const int32_t *index_i, const int32_t *index_j, const int32_t *index_k,
+                       const int32_t *index_l, int64_t *ind2_pp, int64_t *ind3_pp, int64_t *ind4_pp,
+                       double *gamma_pp, int64_t *ind2_pm, int64_t *ind3_pm, int64_t *ind4_pm, double *gamma_pm,
+                       int64_t *ind2_mm, int64_t *ind3_mm, int64_t *ind4_mm, double *gamma_mm, double *rate_4ph,
+                       double *rate_plusplus, double *rate_plusminus, double *rate_minusminus,
+                       double *wp4_plusplus, double *wp4_plusminus, double *wp4_minusminus);
+
+/*
  * Replaces iteration0 (Src/iterations.f90:13-30).
  * allequilist(nsymm_rot,*) as ALLEquiList; F_n(nbands,nptk,3).
  */
@@ -179,6 +198,25 @@ int fp4_iteration(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32
                   const int32_t *ind2_minus, const int32_t *ind3_minus, const double *omega,
                   const double *velocity, const double *gamma_plus, const double *gamma_minus,
                   const double *tau_zero, double *f_n);
+
+/*
+ * Replaces iteration_4ph (Src/iterations.f90:95-215): the sweep of
+ * fp4_iteration with the ++, +- and -- lists of fp4_ind_driver_4ph added
+ * (Gamma times F_l-F_j-F_k, F_l-F_j+F_k and F_l+F_j+F_k respectively).
+ */
+int fp4_iteration_4ph(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32_t *nequi,
+                      const int32_t *allequilist, const int32_t *typeofsymmetry, int32_t nsymm_rot,
+                      const int32_t *id_equi, const double *symmetrizers, const int32_t *n_plus,
+                      const int32_t *n_minus, int32_t ntotal_plus, int32_t ntotal_minus, const int64_t *n_plusplus,
+                      const int64_t *n_plusminus, const int64_t *n_minusminus, int64_t ntotal_plusplus,
+                      int64_t ntotal_plusminus, int64_t ntotal_minusminus, const int32_t *ind2_plus,
+                      const int32_t *ind3_plus, const int32_t *ind2_minus, const int32_t *ind3_minus,
+                      const int64_t *ind2_pp, const int64_t *ind3_pp, const int64_t *ind4_pp,
+                      const int64_t *ind2_pm, const int64_t *ind3_pm, const int64_t *ind4_pm,
+                      const int64_t *ind2_mm, const int64_t *ind3_mm, const int64_t *ind4_mm, const double *omega,
+                      const double *velocity, const double *gamma_plus, const double *gamma_minus,
+                      const double *gamma_pp, const double *gamma_pm, const double *gamma_mm,
+                      const double *tau_zero, double *f_n);
 
 /* F_n(:,q,:) symmetrisation of every q (Src/ShengBTE.f90:1288-1290). */
 int fp4_symmetrize_fn(fp4_ctx *ctx, const fp4_globals *g, const double *symmetrizers, double *f_n);

@@ -444,14 +444,16 @@ void fp4o_ind3(const fp4o_sys *s, const fp4o_ifc *f, const int32_t *n_plus, cons
  *   NP_plusplus/plusminus/minusminus  processes.f90:2263-2476   (mode 0)
  *   Ind_only_plusplus/...             processes.f90:2854-3074   (mode 1)
  *   RTA_plusplus/...                  processes.f90:3828-4129   (mode 2)
- * All three share the loop nest ii, jj, j, k, l with the channel's restrictions.
+ *   Ind_plusplus/plusminus/minusminus processes.f90:3254-3548   (mode 3)
+ * All four share the loop nest ii, jj, j, k, l with the channel's restrictions.
  */
 typedef struct {
     int64_t n;
     double P, gamma, wp;
     int64_t cap;
     int64_t *ind2, *ind3, *ind4;
-    int ii0, ii1; /* optional q' range [ii0, ii1) (0-based); ii1 == 0 means all */
+    double *glist; /* mode 3: Gamma of each listed process */
+    int ii0, ii1;  /* optional q' range [ii0, ii1) (0-based); ii1 == 0 means all */
 } acc4_t;
 
 static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int mode, acc4_t *a) {
@@ -486,7 +488,7 @@ static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int 
                 int ss = index_n(s, qtp);
                 if (ch == 0 ? !(ss >= 1) : !(ss >= jj)) continue;
                 double rqp[3], rqdp[3], rqtp[3];
-                if (mode == 2) {
+                if (mode >= 2) {
                     realq(s, qp, rqp);
                     realq(s, qdp, rqdp);
                     realq(s, qtp, rqtp);
@@ -521,6 +523,31 @@ static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int 
                                 continue;
                             }
                             if (sigma <= floor_sigma) sigma = 1 / sqrt(FP4O_PI);
+                            if (mode == 3) {
+                                /* Ind_*: the process's own Gamma, listed in enumeration order */
+                                double f1 = fbe(s, omegap), f2 = fbe(s, omegadp), f3 = fbe(s, omegatp);
+                                double bose = (ch == 0)   ? (f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3)
+                                              : (ch == 1) ? (f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3)
+                                                          : ((1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3);
+                                double wp4 = bose * exp(-(delta * delta) / (sigma * sigma)) / sigma /
+                                             sqrt(FP4O_PI) / (omega * omegap * omegadp * omegatp);
+                                if (omegap <= 1.25 || omegadp <= 1.25 || omegatp <= 1.25) wp4 = 0;
+                                a->wp = a->wp + wp4;
+                                double vr, vi;
+                                fp4o_vp4(s, f, ch, i, j, k, l, s->list[ll - 1], ii, jj, ss, rqp, rqdp, rqtp, &vr,
+                                         &vi);
+                                double av = hypot(vr, vi);
+                                double g = hp * hp * FP4O_PI / 8.0 * wp4 * (av * av);
+                                g = g * (double)3.37617087f * 1.e9 / nptk / nptk;
+                                if (a->n < a->cap) {
+                                    a->ind2[a->n] = (int64_t)(ii - 1) * nb + j;
+                                    a->ind3[a->n] = (int64_t)(jj - 1) * nb + k;
+                                    a->ind4[a->n] = (int64_t)(ss - 1) * nb + l;
+                                    a->glist[a->n] = g;
+                                }
+                                a->n++;
+                                continue;
+                            }
                             a->n++;
                             if (mode == 0) {
                                 a->P = a->P + exp(-(delta * delta) / (sigma * sigma)) /
@@ -547,7 +574,7 @@ static void proc4_one(const fp4o_sys *s, const fp4o_ifc *f, int mm, int ch, int 
                 }
             }
         }
-        if (mode == 2) a->wp = a->wp / nptk / nptk;
+        if (mode >= 2) a->wp = a->wp / nptk / nptk;
     }
     if (mode == 2) a->gamma = a->gamma * (double)3.37617087f * 1.e9 / nptk / nptk;
 }
@@ -608,6 +635,45 @@ void fp4o_rta4(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, double *r
         rate_mm[m0] = a.gamma;
         wp_mm[m0] = a.wp;
     }
+}
+
+/*
+ * Ind_driver_4ph (processes.f90:3551-3822): per-process Gamma lists of the
+ * three channels at offsets Naccum(mm) = sum of N(1:mm-1), rate = sum(Gamma0)
+ * in list order, WP4 per mode.  Modes with N(mm) == 0 are skipped, as there.
+ */
+void fp4o_ind4(const fp4o_sys *s, const fp4o_ifc *f, const int64_t *n_pp, const int64_t *n_pm, const int64_t *n_mm,
+               int64_t *i2pp, int64_t *i3pp, int64_t *i4pp, double *g_pp, int64_t *i2pm, int64_t *i3pm,
+               int64_t *i4pm, double *g_pm, int64_t *i2mm, int64_t *i3mm, int64_t *i4mm, double *g_mm,
+               double *rate_pp, double *rate_pm, double *rate_mm, double *wp_pp, double *wp_pm, double *wp_mm) {
+    const int nm = s->nb * s->nlist;
+    const int64_t *N[3] = {n_pp, n_pm, n_mm};
+    int64_t *I2[3] = {i2pp, i2pm, i2mm}, *I3[3] = {i3pp, i3pm, i3mm}, *I4[3] = {i4pp, i4pm, i4mm};
+    double *G[3] = {g_pp, g_pm, g_mm}, *R[3] = {rate_pp, rate_pm, rate_mm}, *W[3] = {wp_pp, wp_pm, wp_mm};
+    int64_t *acc = (int64_t *)calloc((size_t)3 * (nm + 1), sizeof(int64_t));
+    for (int ch = 0; ch < 3; ch++)
+        for (int m = 0; m < nm; m++) acc[ch * (nm + 1) + m + 1] = acc[ch * (nm + 1) + m] + N[ch][m];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int x = 0; x < 3 * nm; x++) {
+        int ch = x % 3, m0 = x / 3;
+        R[ch][m0] = 0.0;
+        W[ch][m0] = 0.0;
+        if (N[ch][m0] == 0) continue;
+        int64_t o = acc[ch * (nm + 1) + m0];
+        acc4_t a;
+        memset(&a, 0, sizeof a);
+        a.cap = N[ch][m0];
+        a.ind2 = I2[ch] + o;
+        a.ind3 = I3[ch] + o;
+        a.ind4 = I4[ch] + o;
+        a.glist = G[ch] + o;
+        proc4_one(s, f, m0 + 1, ch, 3, &a);
+        double sum = 0.0;
+        for (int64_t e = 0; e < N[ch][m0]; e++) sum = sum + a.glist[e];
+        R[ch][m0] = sum;
+        W[ch][m0] = a.wp;
+    }
+    free(acc);
 }
 
 /*

@@ -161,6 +161,25 @@ class Oracle:
         return dict(ind2_plus=i2p, ind3_plus=i3p, gamma_plus=gp, ind2_minus=i2m, ind3_minus=i3m, gamma_minus=gm,
                     rate_plus=outs[0], rate_minus=outs[1], wp3_plus=outs[2], wp3_minus=outs[3])
 
+    def ind4(self, n_pp, n_pm, n_mm):
+        """Ind_driver_4ph: per-process Gamma lists, rates and WP4 of the three channels.
+        Returns a dict usable as the `ind4` argument of iteration()."""
+        nm = self.s.nmodes
+        N = [np.ascontiguousarray(x, np.int64) for x in (n_pp, n_pm, n_mm)]
+        out = dict(n_pp=N[0], n_pm=N[1], n_mm=N[2])
+        args = [ct.byref(self.sys), ct.byref(self.ifc4)] + [_p(x) for x in N]
+        for ch, n in zip(("pp", "pm", "mm"), N):
+            tot = int(n.sum())
+            for key in ("ind2_", "ind3_", "ind4_"):
+                out[key + ch] = np.zeros(tot, np.int64)
+            out["gamma_" + ch] = np.zeros(tot)
+            args += [_p(out["ind2_" + ch]), _p(out["ind3_" + ch]), _p(out["ind4_" + ch]), _p(out["gamma_" + ch])]
+        for key in ("rate_pp", "rate_pm", "rate_mm", "wp_pp", "wp_pm", "wp_mm"):
+            out[key] = np.zeros(nm)
+        args += [_p(out[k]) for k in ("rate_pp", "rate_pm", "rate_mm", "wp_pp", "wp_pm", "wp_mm")]
+        lib().fp4o_ind4(*args)
+        return out
+
     def vp3(self, which, i, j, k, q, qp, qdp):
         rq = self._realq(qp); rqd = self._realq(qdp)
         re = ct.c_double(); im = ct.c_double()
