@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=64)
     return ap.parse_args()
 
 
@@ -434,6 +436,8 @@ def run_ours(args):
                       "d2h_bytes_per_step": int(d2h)}
         ce.close()
 
+    if rank == 0 and world == 1 and not args.no_serve:
+        out["serving"] = run_serving(args)
     peak = fp64_dgemm_peak(torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -477,6 +481,63 @@ def run_ours(args):
 
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------- serving stream
+
+
+def run_serving(args):
+    """A Poisson stream of random-cell 3ph+4ph RTA requests through the serving
+    path (mixed precision, continuous batching), against the same cells
+    solved one at a time through the plain FP64 drivers."""
+    from fourphonon_b200 import abi, serve
+    from fourphonon_b200 import system as S
+
+    pool = S.serving_pool()
+    # serial plain FP64: each pool cell alone, rates + tau + iteration0 + TConduct + symmetrize
+    ctx = abi.Context(0, abi.FP4_PREC_FP64)
+    for s in pool[:2]:  # warm-up (library load, first allocations)
+        ctx.rta_driver(s, T=300.0)
+    k64, times = [], []
+    for s in pool:
+        t0 = time.perf_counter()
+        r3 = ctx.rta_driver(s, T=300.0)
+        r4 = ctx.rta_driver_4ph(s, temperatures=[300.0])
+        rate = r3["rate_plus"] + r3["rate_minus"] + (r4["rate_plusplus"][0] + r4["rate_plusminus"][0]) + \
+            r4["rate_minusminus"][0]
+        tau = np.zeros_like(rate)
+        tau[rate != 0] = 1.0 / rate[rate != 0]
+        F = ctx.iteration0(s, tau)
+        kap = ctx.tconduct(s, F, T=300.0).reshape(3, 3, s.nb).sum(axis=2).T
+        R = s.sym.crotations
+        k64.append(sum(R[r] @ kap @ R[r].T for r in range(len(R))) / len(R))
+        times.append(time.perf_counter() - t0)
+    ctx.close()
+    t_serial = float(np.mean(times))
+    rng = np.random.default_rng(20240604)
+    n = max(len(pool), args.serve_requests)
+    rate = 2.0 / t_serial  # arrivals at twice the serial FP64 capacity
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    reqs = [serve.Request(float(arrivals[i]), pool[i], 300.0, tag=("pool", i)) for i in range(len(pool))]
+    for i in range(len(pool), n):
+        c = int(rng.integers(len(pool)))
+        reqs.append(serve.Request(float(arrivals[i]), pool[c], float(rng.uniform(100.0, 1000.0)), tag=("rand", c)))
+    srv = serve.Server(0, abi.FP4_PREC_MIXED, max_slots=16, max_bands=12, hbm_budget=24 << 30)
+    tick_items = 32768
+    done, summ = serve.run_stream(srv, reqs, tick_items=tick_items)
+    srv.close()
+    kerr = 0.0
+    for r in done:
+        if r.tag[0] == "pool":
+            ref = k64[r.tag[1]]
+            kerr = max(kerr, float(np.abs(r.result["kappa"] - ref).max() / np.abs(ref).max()))
+    return {"requests": n, "solves_per_s": summ["solves_per_s"], "p50_ms": summ["p50_ms"], "p99_ms": summ["p99_ms"],
+            "mean_ms": summ["mean_ms"], "processes_per_s": summ["processes_per_s"], "ticks": summ["ticks"],
+            "serial_fp64_solves_per_s": 1.0 / t_serial, "vs_serial_fp64": summ["solves_per_s"] * t_serial,
+            "kappa_rel_err_max": kerr, "precision": "mixed", "max_slots": 16, "tick_items": tick_items,
+            "arrivals": "Poisson at twice the serial FP64 rate",
+            "workload": f"{len(pool)} random 2-4 atom cells (masses U[6,120] amu, seeded BvK + Gaussian IFCs), "
+                        "grids 4^3-8^3 with nptk*nbands <= 3072, T~U[100,1000] K, 3ph+4ph RTA + kappa"}
 
 
 def main():

@@ -466,6 +466,18 @@ static int run_k3(fp4_ctx* c, int mode, const fp4_globals* g, P3Params& p) {
     return FP4_OK;
 }
 
+// 3-phonon RTA of the context's current system into device memory d_out:
+// rate_plus, rate_minus (with the factor 1/2), WP3_plus, WP3_minus, each nbands*nlist.
+int fp4_launch_rta3(fp4_ctx* c, const fp4_globals* g, double* d_out) {
+    const int nm = c->S.nb * c->S.nlist;
+    P3Params p{};
+    p.rate[0] = d_out;
+    p.rate[1] = d_out + nm;
+    p.wp[0] = d_out + 2 * nm;
+    p.wp[1] = d_out + 3 * nm;
+    return run_k3(c, 2, g, p);
+}
+
 extern "C" int fp4_np_driver(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
                              int32_t nlist, const int32_t* list, const int32_t* ijk, int32_t* n_plus,
                              double* p_plus, int32_t* n_minus, double* p_minus) {
@@ -653,8 +665,8 @@ extern "C" int fp4_ind_driver(fp4_ctx* c, const fp4_globals* g, const double* en
 // ---------------------------------------------------------------------------
 // four-phonon drivers
 // ---------------------------------------------------------------------------
-static int k4_blocks(fp4_ctx* c, int nwork) {
-    int nbk = c->sm_count * k4_ctas_per_sm();
+static int k4_blocks(fp4_ctx* c, int nwork, int kind, int nT) {
+    int nbk = c->sm_count * k4_ctas_per_sm(kind, nT);
     return std::max(1, std::min(nbk, nwork));
 }
 
@@ -678,7 +690,7 @@ static int run_np4(fp4_ctx* c, int64_t* n_out[3], double* p_out[3]) {
     p.stats = c->b_stats.as<unsigned long long>();
     p.err = c->b_err.as<int>();
     CK(cudaEventRecord(c->evk0, c->stream));
-    CK(launch_k4(0, 1, false, p, k4_blocks(c, p.nwork), c->stream));
+    CK(launch_k4(0, 1, false, p, k4_blocks(c, p.nwork, 0, 1), c->stream));
     CK(cudaEventRecord(c->evk1, c->stream));
     c->kernel_timed = true;
     c->launches++;
@@ -789,7 +801,7 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     CK(launch_bose(S, c->b_temps.as<double>(), nT, c->b_bose.as<double>(), c->stream));
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
-    const int nblocks = k4_blocks(c, nwork);
+    const int nblocks = k4_blocks(c, nwork, 2, nT);
     P4Params p{};
     if ((r = k4_queue(c, nblocks, false, p))) return r;
     if ((r = c->b_part.reserve(c, (size_t)nwork * nT * S.nb * 2 * sizeof(double)))) return r;
@@ -922,7 +934,7 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
     CK(launch_bose(S, c->b_temps.as<double>(), 1, c->b_bose.as<double>(), c->stream));
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
-    const int nblocks = k4_blocks(c, nwork);
+    const int nblocks = k4_blocks(c, nwork, 3, 1);
     if ((r = k4_queue(c, nblocks, true, p))) return r;
     if ((r = c->b_part.reserve(c, (size_t)nwork * S.nb * 2 * sizeof(double)))) return r;
     if ((r = c->b_work.reserve(c, 64))) return r;

@@ -242,6 +242,23 @@ __global__ void k_tconduct(int nb, int nptk, double T, double scale, const doubl
 
 }  // namespace
 
+namespace fp4 {
+cudaError_t launch_iteration0(int nb, int nptk, int nlist, int nsr, const int* nequi, const int* allequi,
+                              const double* energy, const double* velocity, const double* tau_zero, double* F,
+                              cudaStream_t st) {
+    k_iteration0<<<256, 256, 0, st>>>(nb, nptk, nlist, nsr, nequi, allequi, energy, velocity, tau_zero, F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tconduct(int nb, int nptk, double T, double V, const double* energy, const double* velocity,
+                            const double* F, double* kappa, cudaStream_t st) {
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    const double scale = (double)1e21f * (hbar * hbar) / (kb * T * T * V * nptk);
+    k_tconduct<<<nb, 256, 0, st>>>(nb, nptk, T, scale, energy, velocity, F, kappa, nullptr);
+    return cudaGetLastError();
+}
+}  // namespace fp4
+
 #define CK(call)                                                                                      \
     do {                                                                                              \
         cudaError_t e_ = (call);                                                                      \

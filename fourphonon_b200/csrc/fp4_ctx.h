@@ -77,3 +77,4 @@ int fp4_begin(fp4_ctx* c);
 int fp4_end(fp4_ctx* c);
 int fp4_setup_system(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
                      const double* eigenvect, int32_t nlist, const int32_t* list, const int32_t* ijk);
+int fp4_launch_rta3(fp4_ctx* c, const fp4_globals* g, double* d_out);

@@ -57,6 +57,15 @@ struct P4Params {
     long long* queue_pos;   // list position of each queued process, same indexing as queue
 };
 
+// One launch of the multi-solve kernel: ranges of work items, each of one solve slot.
+constexpr int kMaxTickRanges = 64;
+struct K4Tick {
+    int nranges;
+    int slot[kMaxTickRanges];
+    int begin[kMaxTickRanges];
+    int prefix[kMaxTickRanges + 1];  // prefix[r]: work items in ranges before r; prefix[nranges] = total
+};
+
 struct P4OrderParams {
     DevSys S;
     int ch;
@@ -74,10 +83,21 @@ size_t k3_smem(int mode, const DevIfc& F, bool onlyharmonic);
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st);
 size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F);
 int k4_threads();
-int k4_ctas_per_sm();
+int k4_ctas_per_sm(int kind, int nT);
+cudaError_t launch_k4_multi(bool mixed, const P4Params* slots, const K4Tick* tick, int* counter,
+                            unsigned long long* queue, double* queue_sigma, int cta_bins, int subcap, size_t smem,
+                            int nblocks, cudaStream_t st);
+size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F);
 cudaError_t launch_k4_reduce(const P4Params& p, double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp,
                              double* wp_pm, double* wp_mm, double rate_scale, cudaStream_t st);
 cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st);
 cudaError_t launch_bose(const DevSys& S, const double* T, int nT, double* bose, cudaStream_t st);
+cudaError_t prepare_k4_multi(bool mixed, size_t smem);
+// fp4_bte.cu: iteration0 and TConduct on device-resident arrays (reference layouts)
+cudaError_t launch_iteration0(int nb, int nptk, int nlist, int nsr, const int* nequi, const int* allequi,
+                              const double* energy, const double* velocity, const double* tau_zero, double* F,
+                              cudaStream_t st);
+cudaError_t launch_tconduct(int nb, int nptk, double T, double V, const double* energy, const double* velocity,
+                            const double* F, double* kappa, cudaStream_t st);
 
 }  // namespace fp4

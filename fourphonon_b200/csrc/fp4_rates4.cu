@@ -31,10 +31,14 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity checks
-#ifndef FP4_K4_CTAS_PER_SM
-#define FP4_K4_CTAS_PER_SM 2
-#endif
-constexpr int kCtasPerSm = FP4_K4_CTAS_PER_SM;  // resident persistent CTAs per SM (register budget)
+// Resident persistent CTAs per SM, which sets the register budget.  Three CTAs
+// (80 registers) suit the one- and two-temperature kernels: on the 16^3 diamond
+// workload the FP32 contraction runs 1.21x and the FP64 one 1.01x faster than
+// with two.  Four or more temperatures keep two CTAs, where three would spill.
+template <int KIND, int NT>
+constexpr int ctas_per_sm() {
+    return (KIND != 0 && NT >= 4) ? 2 : 3;
+}
 
 template <bool MIXED>
 struct CT;
@@ -399,30 +403,36 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
     k4_phase_b<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
 }
 
-template <int KIND, int NT, bool MIXED>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) k4_work(P4Params p) {
+// Per-thread work counters of one kernel, flushed into a P4Params::stats array.
+struct K4Stats {
+    unsigned long long surv, contr, sig, cand;
+};
+
+__device__ __forceinline__ void k4_flush_stats(unsigned long long* stats, K4Stats& st, double* red) {
+    double v[4] = {(double)st.surv, (double)st.contr, (double)st.sig, (double)st.cand};
+    block_sum_vec<4>(v, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&stats[0], (unsigned long long)v[0]);
+        atomicAdd(&stats[1], (unsigned long long)v[1]);
+        atomicAdd(&stats[2], (unsigned long long)v[2]);
+        atomicAdd(&stats[3], (unsigned long long)v[3]);
+    }
+    st = K4Stats{0, 0, 0, 0};
+}
+
+// Per-CTA tables of one solve: (k,l) decode table, non-empty class blocks and
+// per-class phase tables.
+template <int KIND, bool MIXED>
+__device__ void k4_cta_init(const P4Params& p, unsigned char* smem, const Layout& L) {
     using C = CT<MIXED>;
     using cx = typename C::T;
-    extern __shared__ __align__(16) unsigned char smem[];
     const DevSys& S = p.S;
     const DevIfc& F = p.F;
-    const int nb = S.nb, nptk = S.nptk, nb2 = nb * nb, npi = F.npi;
+    const int nb = S.nb, nb2 = nb * nb, npi = F.npi;
     const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2], lsum = N0 + N1 + N2;
-    const Layout L = k4_layout(KIND, NT, MIXED, nb, npi, F.ntri, lsum);
-    double2* kap = reinterpret_cast<double2*>(smem + L.kap);
     cx* PT = reinterpret_cast<cx*>(smem + L.pt);
-    double* sval = reinterpret_cast<double*>(smem + L.sval);
-    double* racc = reinterpret_cast<double*>(smem + L.racc);
-    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
-    double* pacc = reinterpret_cast<double*>(smem + L.pacc);
-    double* red = reinterpret_cast<double*>(smem + L.red);
-    int* sidx = reinterpret_cast<int*>(smem + L.sidx);
-    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
-    int* ncnt = reinterpret_cast<int*>(smem + L.ncnt);
     int* klt = reinterpret_cast<int*>(smem + L.klt);
     int* misc = reinterpret_cast<int*>(smem + L.misc);
-
-    // once per CTA: (k,l) decode table, non-empty class blocks and per-class phase tables
     for (int x = threadIdx.x; x < nb2; x += blockDim.x) klt[x] = ((x / nb) << 8) | (x % nb);
     if (threadIdx.x == 0) {
         int4* blkinfo = reinterpret_cast<int4*>(smem + L.blk);
@@ -445,186 +455,263 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k4_work(P4Params p) {
     }
     __syncthreads();
 
+}
+
+// One work item (q = List(ll), q', channel) of one solve.
+template <int KIND, int NT, bool MIXED>
+__device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, const Layout& L, int wi,
+                                        unsigned long long* qbase, double* qsig, long long* qpos, K4Stats& st) {
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const int nb = S.nb, nptk = S.nptk, nb2 = nb * nb;
+    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2];
+    double2* kap = reinterpret_cast<double2*>(smem + L.kap);
+    double* sval = reinterpret_cast<double*>(smem + L.sval);
+    double* racc = reinterpret_cast<double*>(smem + L.racc);
+    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
+    double* pacc = reinterpret_cast<double*>(smem + L.pacc);
+    int* sidx = reinterpret_cast<int*>(smem + L.sidx);
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* ncnt = reinterpret_cast<int*>(smem + L.ncnt);
+    int* klt = reinterpret_cast<int*>(smem + L.klt);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+    constexpr bool LIST = (KIND == 3);
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const double floor_sigma = (double)0.001f;
+    unsigned long long& my_surv = st.surv;
+    unsigned long long& my_contr = st.contr;
+    unsigned long long& my_sig = st.sig;
+    unsigned long long& my_cand = st.cand;
+    const int ch = wi % 3;
+    const int rest = wi / 3;
+    const int ii = rest % nptk, ll = rest / nptk;
+    const int q0 = S.list0[ll];
+    int n0, n1, n2, m0, m1, m2;
+    q_coords_t(S, q0, n0, n1, n2);
+    q_coords_t(S, ii, m0, m1, m2);
+    // sorted branch sums s_ij = w_i +- w'_j over the valid pairs
+    for (int idx = threadIdx.x; idx < nb2; idx += blockDim.x) {
+        int i = idx / nb, j = idx % nb;
+        double wi_ = S.wv[q0 * nb + i].w, wj_ = S.wv[ii * nb + j].w;
+        bool ok = (wi_ != 0.0) && (wi_ <= S.omega_max) && (wj_ != 0.0);
+        double s = (ch == 2) ? __dadd_rn(wi_, -wj_) : __dadd_rn(wi_, wj_);
+        int rank = 0, nvalid = 0;
+        for (int y = 0; y < nb2; y++) {
+            int iy = y / nb, jy = y % nb;
+            double wiy = S.wv[q0 * nb + iy].w, wjy = S.wv[ii * nb + jy].w;
+            bool oky = (wiy != 0.0) && (wiy <= S.omega_max) && (wjy != 0.0);
+            if (!oky) continue;
+            nvalid++;
+            double sy = (ch == 2) ? __dadd_rn(wiy, -wjy) : __dadd_rn(wiy, wjy);
+            if (sy < s || (sy == s && y < idx)) rank++;
+        }
+        if (ok) {
+            sval[rank] = s;
+            sidx[rank] = idx;
+        }
+        if (idx == 0) misc[1] = nvalid;
+        cnt[idx] = 0;
+    }
+    for (int x = threadIdx.x; x < nb; x += blockDim.x) {
+        ncnt[x] = 0;
+        pacc[x] = 0.0;
+    }
+    for (int x = threadIdx.x; x < nb * NT; x += blockDim.x) {
+        racc[x] = 0.0;
+        wacc[x] = 0.0;
+    }
+    if (KIND >= 2) {
+        // kappa_c = mu_c exp(2 pi i (-n.m_l +- n'.(m_j - m_l))/N)
+        for (int c = threadIdx.x; c < F.ntri; c += blockDim.x) {
+            int4 mj = F.mj[c], ml = F.ml[c];
+            double2 a = lattice_phase(S, n0, n1, n2, -ml.x, -ml.y, -ml.z);
+            int sj = (ch == 2) ? -1 : 1;
+            double2 b = lattice_phase(S, m0, m1, m2, sj * (mj.x - ml.x), sj * (mj.y - ml.y), sj * (mj.z - ml.z));
+            double2 k = cmul(a, b);
+            k.x *= F.mu[c];
+            k.y *= F.mu[c];
+            kap[c] = k;
+        }
+    }
+    __syncthreads();
+    const int ns = misc[1];
+    if (KIND == 3) {
+        k4_list_segment<NT, MIXED>(p, smem, L, qbase, qsig, qpos, ch, ii, ll, q0, m0, m1, m2, n0, n1, n2, my_surv,
+                                   my_contr);
+    } else if (ns > 0) {
+        double smax = 0.0;
+        for (int x = 0; x < ns; x++) smax = fmax(smax, fabs(sval[x]));
+        const int jj_lo = (ch == 1) ? 0 : ii;
+        const int total = (nptk - jj_lo) * nb2;
+        // thread t covers index base+t; keep (jj, kl) of it incrementally
+        const int Bq = blockDim.x / nb2, Br = blockDim.x % nb2;
+        int cj = threadIdx.x / nb2, ckl = threadIdx.x % nb2;
+        int iter = 0;
+        for (int base = 0; base < total; base += blockDim.x, iter++) {
+            if (KIND == 2 && (iter % kCheckEvery) == 0) {
+                if (queue_nearly_full(p, cnt, nb2, misc))
+                    k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                                                my_contr);
+            }
+            if (base + (int)threadIdx.x < total) {
+                const int jj = jj_lo + cj;
+                const int kl = klt[ckl];
+                const int k = kl >> 8, l = kl & 0xff;
+                int a, b, c;
+                q_coords_t(S, jj, a, b, c);
+                int t0, t1, t2;
+                if (ch == 0) {
+                    t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+                } else if (ch == 1) {
+                    t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+                } else {
+                    t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+                }
+                const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
+                bool go = true;
+                if (ch != 0 && ss < jj) go = false;
+                if (ch != 0 && ss == jj && l < k) go = false;
+                if (go) {
+                    const double4 w2 = S.wv[jj * nb + k];
+                    const double4 w3 = S.wv[ss * nb + l];
+                    if (w2.w != 0.0 && w3.w != 0.0) {
+                        const double sigma = sigma_exact(S, w2, w3);
+                        my_sig++;
+                        const double cen = (ch == 0) ? (w3.w - w2.w) : (w2.w + w3.w);
+                        const double tol = 1e-12 * (1.0 + fabs(w2.w) + fabs(w3.w) + smax + sigma);
+                        int x = lower_bound_d(sval, ns, cen - sigma - tol);
+                        for (; x < ns && sval[x] <= cen + sigma + tol; x++) {
+                            my_cand++;
+                            const double s = sval[x];
+                            const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w)
+                                                           : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
+                            if (!(fabs(delta) <= sigma)) continue;
+                            const int idx = sidx[x];
+                            const int i = idx / nb, j = idx - i * nb;
+                            if (ch != 1 && jj == ii && k < j) continue;
+                            if (ch == 1 && !((q0 != jj || i != k) && (q0 != ss || i != l) && (ii != jj || j != k) &&
+                                             (ii != ss || j != l)))
+                                continue;
+                            my_surv++;
+                            if (KIND == 0) {
+                                atomicAdd(&ncnt[i], 1);
+                                const double sg = (sigma <= floor_sigma) ? 1.0 / sqrtpi : sigma;
+                                const double pc = exp(-(delta * delta) / (sg * sg)) /
+                                                  (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
+                                                   (double)(nb * nb * nb * nb));
+                                atomicAdd(&pacc[i], pc);
+                                continue;
+                            }
+                            const double w1 = S.wv[ii * nb + j].w;
+                            if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
+                            const int pos = atomicAdd(&cnt[idx], 1);
+                            qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
+                            qsig[(size_t)idx * p.subcap + pos] = sigma;
+                        }
+                    }
+                }
+            }
+            ckl += Br;
+            cj += Bq;
+            if (ckl >= nb2) {
+                ckl -= nb2;
+                cj += 1;
+            }
+        }
+        if (KIND == 2) {
+            __syncthreads();
+            k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                                        my_contr);
+        }
+    }
+    __syncthreads();
+    if (KIND == 0) {
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+            if (ncnt[i]) atomicAdd(&p.n_count[ch * S.nlist * nb + ll * nb + i], (unsigned long long)ncnt[i]);
+            if (pacc[i] != 0.0) atomicAdd(&p.p_sum[ch * S.nlist * nb + ll * nb + i], pacc[i]);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < nb * NT; idx += blockDim.x) {
+            int i = idx / NT, t = idx % NT;
+            if (t < p.nT) {
+                p.part_rate[((size_t)wi * p.nT + t) * nb + i] = racc[idx];
+                p.part_wp[((size_t)wi * p.nT + t) * nb + i] = wacc[idx];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int KIND, int NT, bool MIXED>
+__global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT>())) k4_work(P4Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nb2 = p.S.nb * p.S.nb;
+    const Layout L = k4_layout(KIND, NT, MIXED, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2]);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+    k4_cta_init<KIND, MIXED>(p, smem, L);
     unsigned long long* qbase = p.queue + (size_t)blockIdx.x * nb2 * p.subcap;
     double* qsig = p.queue_sigma + (size_t)blockIdx.x * nb2 * p.subcap;
     long long* qpos = (KIND == 3) ? p.queue_pos + (size_t)blockIdx.x * nb2 * p.subcap : nullptr;
-    constexpr bool LIST = (KIND == 3);
-    unsigned long long my_surv = 0, my_contr = 0, my_sig = 0, my_cand = 0;
-    const double sqrtpi = sqrt(3.141592653589793238);
-    const double floor_sigma = (double)0.001f;
-
+    K4Stats st{0, 0, 0, 0};
     for (;;) {
         if (threadIdx.x == 0) misc[0] = atomicAdd(p.work_counter, 1);
         __syncthreads();
         const int wi = misc[0];
         if (wi >= p.nwork) break;
-        const int ch = wi % 3;
-        const int rest = wi / 3;
-        const int ii = rest % nptk, ll = rest / nptk;
-        const int q0 = S.list0[ll];
-        int n0, n1, n2, m0, m1, m2;
-        q_coords_t(S, q0, n0, n1, n2);
-        q_coords_t(S, ii, m0, m1, m2);
-        // sorted branch sums s_ij = w_i +- w'_j over the valid pairs
-        for (int idx = threadIdx.x; idx < nb2; idx += blockDim.x) {
-            int i = idx / nb, j = idx % nb;
-            double wi_ = S.wv[q0 * nb + i].w, wj_ = S.wv[ii * nb + j].w;
-            bool ok = (wi_ != 0.0) && (wi_ <= S.omega_max) && (wj_ != 0.0);
-            double s = (ch == 2) ? __dadd_rn(wi_, -wj_) : __dadd_rn(wi_, wj_);
-            int rank = 0, nvalid = 0;
-            for (int y = 0; y < nb2; y++) {
-                int iy = y / nb, jy = y % nb;
-                double wiy = S.wv[q0 * nb + iy].w, wjy = S.wv[ii * nb + jy].w;
-                bool oky = (wiy != 0.0) && (wiy <= S.omega_max) && (wjy != 0.0);
-                if (!oky) continue;
-                nvalid++;
-                double sy = (ch == 2) ? __dadd_rn(wiy, -wjy) : __dadd_rn(wiy, wjy);
-                if (sy < s || (sy == s && y < idx)) rank++;
-            }
-            if (ok) {
-                sval[rank] = s;
-                sidx[rank] = idx;
-            }
-            if (idx == 0) misc[1] = nvalid;
-            cnt[idx] = 0;
-        }
-        for (int x = threadIdx.x; x < nb; x += blockDim.x) {
-            ncnt[x] = 0;
-            pacc[x] = 0.0;
-        }
-        for (int x = threadIdx.x; x < nb * NT; x += blockDim.x) {
-            racc[x] = 0.0;
-            wacc[x] = 0.0;
-        }
-        if (KIND >= 2) {
-            // kappa_c = mu_c exp(2 pi i (-n.m_l +- n'.(m_j - m_l))/N)
-            for (int c = threadIdx.x; c < F.ntri; c += blockDim.x) {
-                int4 mj = F.mj[c], ml = F.ml[c];
-                double2 a = lattice_phase(S, n0, n1, n2, -ml.x, -ml.y, -ml.z);
-                int sj = (ch == 2) ? -1 : 1;
-                double2 b = lattice_phase(S, m0, m1, m2, sj * (mj.x - ml.x), sj * (mj.y - ml.y), sj * (mj.z - ml.z));
-                double2 k = cmul(a, b);
-                k.x *= F.mu[c];
-                k.y *= F.mu[c];
-                kap[c] = k;
-            }
-        }
-        __syncthreads();
-        const int ns = misc[1];
-        if (KIND == 3) {
-            k4_list_segment<NT, MIXED>(p, smem, L, qbase, qsig, qpos, ch, ii, ll, q0, m0, m1, m2, n0, n1, n2, my_surv,
-                                       my_contr);
-        } else if (ns > 0) {
-            double smax = 0.0;
-            for (int x = 0; x < ns; x++) smax = fmax(smax, fabs(sval[x]));
-            const int jj_lo = (ch == 1) ? 0 : ii;
-            const int total = (nptk - jj_lo) * nb2;
-            // thread t covers index base+t; keep (jj, kl) of it incrementally
-            const int Bq = blockDim.x / nb2, Br = blockDim.x % nb2;
-            int cj = threadIdx.x / nb2, ckl = threadIdx.x % nb2;
-            int iter = 0;
-            for (int base = 0; base < total; base += blockDim.x, iter++) {
-                if (KIND == 2 && (iter % kCheckEvery) == 0) {
-                    if (queue_nearly_full(p, cnt, nb2, misc))
-                        k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
-                                                    my_contr);
-                }
-                if (base + (int)threadIdx.x < total) {
-                    const int jj = jj_lo + cj;
-                    const int kl = klt[ckl];
-                    const int k = kl >> 8, l = kl & 0xff;
-                    int a, b, c;
-                    q_coords_t(S, jj, a, b, c);
-                    int t0, t1, t2;
-                    if (ch == 0) {
-                        t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
-                    } else if (ch == 1) {
-                        t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
-                    } else {
-                        t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
-                    }
-                    const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
-                    bool go = true;
-                    if (ch != 0 && ss < jj) go = false;
-                    if (ch != 0 && ss == jj && l < k) go = false;
-                    if (go) {
-                        const double4 w2 = S.wv[jj * nb + k];
-                        const double4 w3 = S.wv[ss * nb + l];
-                        if (w2.w != 0.0 && w3.w != 0.0) {
-                            const double sigma = sigma_exact(S, w2, w3);
-                            my_sig++;
-                            const double cen = (ch == 0) ? (w3.w - w2.w) : (w2.w + w3.w);
-                            const double tol = 1e-12 * (1.0 + fabs(w2.w) + fabs(w3.w) + smax + sigma);
-                            int x = lower_bound_d(sval, ns, cen - sigma - tol);
-                            for (; x < ns && sval[x] <= cen + sigma + tol; x++) {
-                                my_cand++;
-                                const double s = sval[x];
-                                const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w)
-                                                               : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
-                                if (!(fabs(delta) <= sigma)) continue;
-                                const int idx = sidx[x];
-                                const int i = idx / nb, j = idx - i * nb;
-                                if (ch != 1 && jj == ii && k < j) continue;
-                                if (ch == 1 && !((q0 != jj || i != k) && (q0 != ss || i != l) && (ii != jj || j != k) &&
-                                                 (ii != ss || j != l)))
-                                    continue;
-                                my_surv++;
-                                if (KIND == 0) {
-                                    atomicAdd(&ncnt[i], 1);
-                                    const double sg = (sigma <= floor_sigma) ? 1.0 / sqrtpi : sigma;
-                                    const double pc = exp(-(delta * delta) / (sg * sg)) /
-                                                      (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
-                                                       (double)(nb * nb * nb * nb));
-                                    atomicAdd(&pacc[i], pc);
-                                    continue;
-                                }
-                                const double w1 = S.wv[ii * nb + j].w;
-                                if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
-                                const int pos = atomicAdd(&cnt[idx], 1);
-                                qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
-                                qsig[(size_t)idx * p.subcap + pos] = sigma;
-                            }
-                        }
-                    }
-                }
-                ckl += Br;
-                cj += Bq;
-                if (ckl >= nb2) {
-                    ckl -= nb2;
-                    cj += 1;
-                }
-            }
-            if (KIND == 2) {
-                __syncthreads();
-                k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
-                                            my_contr);
-            }
-        }
-        __syncthreads();
-        if (KIND == 0) {
-            for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-                if (ncnt[i]) atomicAdd(&p.n_count[ch * S.nlist * nb + ll * nb + i], (unsigned long long)ncnt[i]);
-                if (pacc[i] != 0.0) atomicAdd(&p.p_sum[ch * S.nlist * nb + ll * nb + i], pacc[i]);
-            }
-        } else {
-            for (int idx = threadIdx.x; idx < nb * NT; idx += blockDim.x) {
-                int i = idx / NT, t = idx % NT;
-                if (t < p.nT) {
-                    p.part_rate[((size_t)wi * p.nT + t) * nb + i] = racc[idx];
-                    p.part_wp[((size_t)wi * p.nT + t) * nb + i] = wacc[idx];
-                }
-            }
-        }
-        __syncthreads();
+        k4_item<KIND, NT, MIXED>(p, smem, L, wi, qbase, qsig, qpos, st);
     }
-    double st[4] = {(double)my_surv, (double)my_contr, (double)my_sig, (double)my_cand};
-    block_sum_vec<4>(st, red);
-    if (threadIdx.x == 0) {
-        atomicAdd(&p.stats[0], (unsigned long long)st[0]);
-        atomicAdd(&p.stats[1], (unsigned long long)st[1]);
-        atomicAdd(&p.stats[2], (unsigned long long)st[2]);
-        atomicAdd(&p.stats[3], (unsigned long long)st[3]);
+    k4_flush_stats(p.stats, st, reinterpret_cast<double*>(smem + L.red));
+}
+
+// Several solves in one persistent launch (the serving path).  The tick lists
+// ranges of work items, each of one solve slot; a CTA that moves to another
+// slot flushes its counters, loads that slot's parameters into shared memory
+// and rebuilds its per-CTA tables.  The queue is per CTA, sized for the largest
+// branch count the server admits.
+template <int NT, bool MIXED>
+__global__ void __launch_bounds__(kThreads, (ctas_per_sm<2, NT>())) k4_work_multi(const P4Params* slots, const K4Tick* tick,
+                                                                                int* counter, unsigned long long* queue,
+                                                                                double* queue_sigma, int cta_bins,
+                                                                                int subcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ P4Params sp;
+    __shared__ int s_slot, s_wi;
+    unsigned long long* qbase = queue + (size_t)blockIdx.x * cta_bins * subcap;
+    double* qsig = queue_sigma + (size_t)blockIdx.x * cta_bins * subcap;
+    K4Stats st{0, 0, 0, 0};
+    int cur = -1;
+    Layout L{};
+    const int total = tick->prefix[tick->nranges];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int g = atomicAdd(counter, 1);
+            int slot = -1, wi = 0;
+            if (g < total) {
+                int r = 0;
+                while (r + 1 < tick->nranges && tick->prefix[r + 1] <= g) r++;
+                slot = tick->slot[r];
+                wi = tick->begin[r] + (g - tick->prefix[r]);
+            }
+            s_slot = slot;
+            s_wi = wi;
+        }
+        __syncthreads();
+        const int slot = s_slot, wi = s_wi;
+        if (slot < 0) break;
+        if (slot != cur) {
+            if (cur >= 0) k4_flush_stats(sp.stats, st, reinterpret_cast<double*>(smem + L.red));
+            __syncthreads();
+            const int* src = reinterpret_cast<const int*>(slots + slot);
+            int* dst = reinterpret_cast<int*>(&sp);
+            for (int x = threadIdx.x; x < (int)(sizeof(P4Params) / sizeof(int)); x += blockDim.x) dst[x] = src[x];
+            __syncthreads();
+            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2]);
+            k4_cta_init<2, MIXED>(sp, smem, L);
+            cur = slot;
+        }
+        k4_item<2, NT, MIXED>(sp, smem, L, wi, qbase, qsig, nullptr, st);
     }
+    if (cur >= 0) k4_flush_stats(sp.stats, st, reinterpret_cast<double*>(smem + L.red));
 }
 
 }  // namespace
@@ -679,7 +766,11 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
-int k4_ctas_per_sm() { return kCtasPerSm; }
+int k4_ctas_per_sm(int kind, int nT) {
+    if (kind == 0) return ctas_per_sm<0, 1>();
+    const int NT = round_nt(nT);
+    return NT >= 4 ? ctas_per_sm<2, 4>() : ctas_per_sm<2, 1>();
+}
 
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st) {
     if (kind == 0) return launch_k4_t<0, 1, false>(p, nblocks, st);
@@ -696,6 +787,25 @@ cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nbloc
     FP4_K4(8)
 #undef FP4_K4
     return cudaErrorInvalidValue;
+}
+
+size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F) { return k4_smem(2, 1, mixed, S, F); }
+
+cudaError_t prepare_k4_multi(bool mixed, size_t smem) {
+    return mixed ? cudaFuncSetAttribute(k4_work_multi<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                 : cudaFuncSetAttribute(k4_work_multi<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// The caller sets the dynamic shared-memory limit once with prepare_k4_multi (so the
+// launch can be captured into a graph).
+cudaError_t launch_k4_multi(bool mixed, const P4Params* slots, const K4Tick* tick, int* counter,
+                            unsigned long long* queue, double* queue_sigma, int cta_bins, int subcap, size_t smem,
+                            int nblocks, cudaStream_t st) {
+    if (mixed)
+        k4_work_multi<1, true><<<nblocks, kThreads, smem, st>>>(slots, tick, counter, queue, queue_sigma, cta_bins, subcap);
+    else
+        k4_work_multi<1, false><<<nblocks, kThreads, smem, st>>>(slots, tick, counter, queue, queue_sigma, cta_bins, subcap);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_k4_reduce(const P4Params& p, double* r0, double* r1, double* r2, double* w0, double* w1, double* w2,

@@ -166,6 +166,28 @@ def layered_solve(ngrid=(12, 12, 12), temperatures=(300.0,), seed=20240602, **kw
     return build_solve(C.layered_rhombohedral(), ngrid, temperatures, seed, fc3_shell=3, fc4_shell=2, **kw)
 
 
+def random_solve(natoms=2, ngrid=(6, 6, 6), temperatures=(300.0,), seed=1, **kw) -> Solve:
+    """A random 2-8 atom cell (crystal.random_cell: masses U[6,120] amu) with the
+    same seeded BvK + Gaussian cluster generator; the request cells of serving."""
+    cr = C.random_cell(np.random.default_rng(seed), natoms)
+    return build_solve(cr, ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, **kw)
+
+
+def serving_pool(n=8, seed=4242, grids=(4, 6, 8), natoms=(2, 3, 4), max_cost=8 ** 3 * 6):
+    """n cached random solves for a request stream: cells of natoms atoms on
+    grids drawn from `grids`, keeping nptk * nbands <= max_cost so that one
+    solve stays a short request."""
+    rng = np.random.default_rng(seed)
+    pool = []
+    while len(pool) < n:
+        na = int(rng.choice(natoms))
+        g = int(rng.choice(grids))
+        if g ** 3 * 3 * na > max_cost:
+            continue
+        pool.append(cached_solve(f"random{na}", (g, g, g), (300.0,), seed=int(rng.integers(1, 1 << 30))))
+    return pool
+
+
 # ---------------------------------------------------------------------------
 # compact on-disk form (npz) for fixtures and caches
 # ---------------------------------------------------------------------------
@@ -223,9 +245,12 @@ def cached_solve(kind: str = "diamond", ngrid=(4, 4, 4), temperatures=(300.0,), 
     if os.path.exists(fn):
         s = load_solve(fn)
     else:
-        builder = {"diamond": diamond_solve, "zincblende": zincblende_solve, "layered": layered_solve}[kind]
         kw = {} if seed is None else {"seed": seed}
-        s = builder(ngrid=tuple(ngrid), temperatures=tuple(temperatures), **kw)
+        if kind.startswith("random"):
+            s = random_solve(int(kind[6:]), ngrid=tuple(ngrid), temperatures=tuple(temperatures), **kw)
+        else:
+            builder = {"diamond": diamond_solve, "zincblende": zincblende_solve, "layered": layered_solve}[kind]
+            s = builder(ngrid=tuple(ngrid), temperatures=tuple(temperatures), **kw)
         tmp = fn + f".{os.getpid()}.tmp.npz"
         save_solve(tmp, s)
         os.replace(tmp, fn)

@@ -284,6 +284,56 @@ int fp4_set_stream(fp4_ctx *ctx, void *stream);
  */
 int fp4_set_upload_cache(fp4_ctx *ctx, int enable);
 
+/*
+ * Serving: many 3ph+4ph RTA solves resident on one GPU.  No counterpart in
+ * the reference, which runs one solve per process.
+ *
+ * fp4_server_create reserves the work queues (sized for max_bands branches)
+ * and captures the tick graph.  On failure *srv may still hold a server whose
+ * fp4_server_last_error explains the failure; destroy it.  hbm_budget_bytes
+ * bounds the queues plus the footprints of the admitted solves.
+ *
+ * fp4_server_admit uploads one solve into a free slot: the arrays of
+ * fp4_rta_driver (3ph) and fp4_rta_driver_4ph (4ph), at g->T, plus the
+ * wedge's Nequi, ALLEquiList(nsymm_rot,nlist), crotations(3,3,nsymm_rot) and
+ * the cell volume (nm^3) for kappa.  It returns FP4_E_STATE when no slot is
+ * free or the budget is in use (retry after a collect), FP4_E_CAPACITY when
+ * the solve can never fit.
+ *
+ * fp4_server_tick runs up to max_items work items (q, q', channel), shared
+ * equally among the running solves, in one launch of the multi-solve kernel,
+ * finishes the solves whose work is complete (rates, tau, iteration0,
+ * TConduct, symmetrised kappa) and lists their slots in finished[] (room for
+ * max_slots entries).  It returns when the tick has run.
+ *
+ * fp4_server_collect copies a finished slot's results (each pointer may be
+ * NULL): rate_plus/rate_minus (3ph; minus with the factor 1/2), the three 4ph
+ * rates (nbands*nlist each), kappa per branch (nbands x 3x3, column-major
+ * blocks), kappa (3x3) and the number of surviving 3ph+4ph processes, then
+ * frees the slot.
+ */
+typedef struct fp4_server fp4_server;
+int fp4_server_create(fp4_server **srv, int device, int precision, int32_t max_slots, int32_t max_bands,
+                      int64_t hbm_budget_bytes);
+int fp4_server_destroy(fp4_server *srv);
+const char *fp4_server_last_error(const fp4_server *srv);
+int64_t fp4_server_footprint(int32_t nbands, int32_t nlist, const int32_t ngrid[3], int32_t ntri3, int32_t ntri4,
+                             int32_t nsymm_rot);
+int fp4_server_admit(fp4_server *srv, const fp4_globals *g, const double *energy, const double *velocity,
+                     const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk, int32_t ntri3,
+                     const double *phi, const double *r_j3, const double *r_k3, const int32_t *index_i3,
+                     const int32_t *index_j3, const int32_t *index_k3, int32_t ntri4, const double *psi,
+                     const double *r_j4, const double *r_k4, const double *r_l4, const int32_t *index_i4,
+                     const int32_t *index_j4, const int32_t *index_k4, const int32_t *index_l4, int32_t nsymm_rot,
+                     const int32_t *nequi, const int32_t *allequilist, const double *crotations, double volume,
+                     int32_t *slot);
+int fp4_server_tick(fp4_server *srv, int64_t max_items, int32_t *finished, int32_t *nfinished);
+int fp4_server_collect(fp4_server *srv, int32_t slot, double *rate3_plus, double *rate3_minus, double *rate4_pp,
+                       double *rate4_pm, double *rate4_mm, double *kappa_branch, double *kappa,
+                       int64_t *n_processes);
+int fp4_server_status(const fp4_server *srv, int32_t *running, int32_t *done, int64_t *bytes_in_use,
+                      double *last_tick_ms, int64_t *ticks);
+
 #ifdef __cplusplus
 }
 #endif
