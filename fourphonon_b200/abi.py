@@ -31,6 +31,12 @@ _lib = None
 
 FP4_PREC_FP64 = 0
 FP4_PREC_MIXED = 1
+FP4_OK = 0
+FP4_E_ARG = -1
+FP4_E_CUDA = -2
+FP4_E_CAPACITY = -3
+FP4_E_TIMEOUT = -4
+FP4_E_STATE = -5
 
 
 class FP4Error(RuntimeError):
@@ -342,6 +348,16 @@ class Context:
         symm = np.ascontiguousarray(np.transpose(s.sym.symmetrizers, (0, 2, 1))).ravel()
         self._chk(self.lib.fp4_symmetrize_fn(self.h, ct.byref(g), _p(symm), _p(F)))
         return F
+
+    def cumulative_tconduct(self, s, F, T=None, nticks=100, omega_mode=False):
+        """CumulativeTConduct (or CumulativeTConductOmega): (ticks, results(nb,3,3,nticks) flat)."""
+        g = self.globals_of(s, T)
+        e, v, _, _, _ = self._arrays(s)
+        ticks = np.zeros(nticks)
+        res = np.zeros(s.nb * 9 * nticks)
+        fn = self.lib.fp4_cumulative_tconduct_omega if omega_mode else self.lib.fp4_cumulative_tconduct
+        self._chk(fn(self.h, ct.byref(g), ct.c_double(s.volume), _p(e), _p(v), _p(F), nticks, _p(ticks), _p(res)))
+        return ticks, res
 
     def tconduct(self, s, F, T=None, with_modes=False):
         g = self.globals_of(s, T)

@@ -666,7 +666,7 @@ extern "C" int fp4_ind_driver(fp4_ctx* c, const fp4_globals* g, const double* en
 // four-phonon drivers
 // ---------------------------------------------------------------------------
 static int k4_blocks(fp4_ctx* c, int nwork, int kind, int nT) {
-    int nbk = c->sm_count * k4_ctas_per_sm(kind, nT);
+    int nbk = c->sm_count * k4_ctas_per_sm(kind, nT, c->precision == FP4_PREC_MIXED);
     return std::max(1, std::min(nbk, nwork));
 }
 

@@ -11,6 +11,8 @@
 // F_n(nbands,nptk,3).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "../../include/fourphonon_b200.h"
@@ -237,6 +239,71 @@ __global__ void k_tconduct(int nb, int nptk, double T, double scale, const doubl
         double t = 0.0;
         for (int w = 0; w < nwarp; w++) t += red[threadIdx.x][w];
         kappa[threadIdx.x * nb + jj] = scale * t;  // ThConductivity(jj,d1,d2): [(d2*3+d1)*nb + jj]
+    }
+}
+
+// Euclidean norm of a 3-vector by the scaled sum of squares of reference BLAS
+// dnrm2, unfused so that it rounds as the host evaluation does.
+__device__ double nrm2_3(double x0, double x1, double x2) {
+    double scale = 0.0, ssq = 1.0;
+    const double x[3] = {x0, x1, x2};
+    for (int i = 0; i < 3; i++) {
+        if (x[i] != 0.0) {
+            const double a = fabs(x[i]);
+            if (scale < a) {
+                const double q = scale / a;
+                ssq = __dadd_rn(1.0, __dmul_rn(__dmul_rn(ssq, q), q));
+                scale = a;
+            } else {
+                const double q = a / scale;
+                ssq = __dadd_rn(ssq, __dmul_rn(q, q));
+            }
+        }
+    }
+    return __dmul_rn(scale, sqrt(ssq));
+}
+
+// CumulativeTConduct / CumulativeTConductOmega (conductivity.f90:64-148): one CTA
+// per (tick, branch) sums the modes whose mean free path (or omega) is below
+// the tick.  results(nb,3,3,nticks) as [((k*3 + d2)*3 + d1)*nb + b].
+__global__ void k_cumulative(int nb, int nptk, int nticks, int omega_mode, double T, double scale,
+                             const double* energy, const double* velocity, const double* F, const double* ticks,
+                             double* results) {
+    __shared__ double red[9][32];
+    const int k = blockIdx.x, jj = blockIdx.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    const double tick = ticks[k];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const size_t pl = (size_t)nptk * nb;
+    for (int ii = 1 + threadIdx.x; ii < nptk; ii += blockDim.x) {  // reference q index 2..nptk
+        const size_t e = (size_t)jj * nptk + ii;
+        const double w = energy[e];
+        const double v[3] = {velocity[e], velocity[e + pl], velocity[e + 2 * pl]};
+        const double f[3] = {F[(size_t)ii * nb + jj], F[((size_t)nptk + ii) * nb + jj], F[((size_t)2 * nptk + ii) * nb + jj]};
+        double lambda;
+        if (omega_mode) {
+            lambda = w;
+        } else {
+            const double dot = __dadd_rn(__dadd_rn(__dmul_rn(f[0], v[0]), __dmul_rn(f[1], v[1])), __dmul_rn(f[2], v[2]));
+            lambda = dot / __dmul_rn(__dadd_rn(w, 1e-12), nrm2_3(v[0], v[1], v[2]));
+        }
+        if (!(tick > lambda)) continue;
+        const double fbe = 1.0 / (exp(hbar * w / kb / T) - 1.0);
+        const double pre = fbe * (fbe + 1) * w;
+        for (int d1 = 0; d1 < 3; d1++)
+            for (int d2 = 0; d2 < 3; d2++) acc[d2 * 3 + d1] += pre * (v[d1] * f[d2]);
+    }
+    for (int x = 0; x < 9; x++) {
+        double t = acc[x];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[x][warp] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        double t = 0.0;
+        for (int w = 0; w < nwarp; w++) t += red[threadIdx.x][w];
+        results[((size_t)k * 9 + threadIdx.x) * nb + jj] = scale * t;
     }
 }
 
@@ -535,4 +602,59 @@ extern "C" int fp4_tconduct(fp4_ctx* c, const fp4_globals* g, double V, const do
     CK(cudaMemcpyAsync(kappa, c->b_out.ptr, nb * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (kmode) CK(cudaMemcpyAsync(kmode, km, (size_t)nptk * nb * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return fp4_end(c);
+}
+
+// CumulativeTConduct (omega_mode 0) and CumulativeTConductOmega (1).
+static int run_cumulative(fp4_ctx* c, const fp4_globals* g, double V, const double* omega, const double* velocity,
+                          const double* f_n, int32_t nticks, double* ticks, double* results, int omega_mode) {
+    if (!c) return FP4_E_ARG;
+    int r;
+    if ((r = check_g(c, g))) return r;
+    if (!omega || !velocity || !f_n || !ticks || !results || !(V > 0.0) || !(g->T > 0.0) || nticks < 2)
+        return fp4_fail(c, FP4_E_ARG, "bad argument");
+    const int nb = g->nbands, nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2];
+    // the thresholds, computed on the host as the reference computes them
+    if (omega_mode == 0) {
+        for (int ii = 1; ii <= nticks; ii++)  // 10.**(8.*(ii-1.)/(nticks-1.)-2.) in default REAL
+            ticks[ii - 1] = (double)powf(10.0f, 8.0f * ((float)ii - 1.0f) / ((float)nticks - 1.0f) - 2.0f);
+    } else {
+        double emin = 1.e10, emax = -1.e10;
+        for (size_t x = 0; x < (size_t)nptk * nb; x++) {
+            emin = std::min(emin, omega[x]);
+            emax = std::max(emax, omega[x]);
+        }
+        emax = emax * 1.1;
+        for (int ii = 1; ii <= nticks; ii++) ticks[ii - 1] = emin + (emax - emin) * ii / nticks;
+    }
+    if ((r = fp4_begin(c))) return r;
+    DevBuffer* B = c->b_bte;
+    if ((r = B[2].upload(c, omega, (size_t)nptk * nb * sizeof(double))) ||
+        (r = B[3].upload(c, velocity, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[5].upload(c, f_n, (size_t)nptk * nb * 3 * sizeof(double))) ||
+        (r = B[9].upload(c, ticks, (size_t)nticks * sizeof(double))) ||
+        (r = c->b_out.reserve(c, (size_t)nb * 9 * nticks * sizeof(double))))
+        return r;
+    const double hbar = 1.05457172647e-22, kb = 1.380648813e-23;
+    const double scale = (double)1e21f * (hbar * hbar) / (kb * g->T * g->T * V * nptk);
+    k_cumulative<<<dim3(nticks, nb), 128, 0, c->stream>>>(nb, nptk, nticks, omega_mode, g->T, scale,
+                                                          B[2].as<double>(), B[3].as<double>(), B[5].as<double>(),
+                                                          B[9].as<double>(), c->b_out.as<double>());
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(results, c->b_out.ptr, (size_t)nb * 9 * nticks * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    B[9].key = 0;
+    return fp4_end(c);
+}
+
+extern "C" int fp4_cumulative_tconduct(fp4_ctx* c, const fp4_globals* g, double V, const double* omega,
+                                       const double* velocity, const double* f_n, int32_t nticks, double* ticks,
+                                       double* results) {
+    return run_cumulative(c, g, V, omega, velocity, f_n, nticks, ticks, results, 0);
+}
+
+extern "C" int fp4_cumulative_tconduct_omega(fp4_ctx* c, const fp4_globals* g, double V, const double* omega,
+                                             const double* velocity, const double* f_n, int32_t nticks,
+                                             double* ticks, double* results) {
+    return run_cumulative(c, g, V, omega, velocity, f_n, nticks, ticks, results, 1);
 }

@@ -153,7 +153,7 @@ extern "C" int fp4_np_driver_4ph_noalloc(const fp4_globals* g, const double* ene
     p.p_sum = ps;
     p.stats = stats;
     p.err = misc + 1;
-    const int nblocks = std::min(k4_ctas_per_sm(0, 1) * sm_count, p.nwork);
+    const int nblocks = std::min(k4_ctas_per_sm(0, 1, false) * sm_count, p.nwork);
     if (launch_k4(0, 1, false, p, nblocks, st) != cudaSuccess) return FP4_E_CUDA;
     k_noalloc_unpack<<<(nm + 255) / 256, 256, 0, st>>>(nm, cnt, ps, n_plusplus, n_plusminus, n_minusminus,
                                                         pspace_plusplus, pspace_plusminus, pspace_minusminus);

@@ -32,12 +32,13 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity checks
 // Resident persistent CTAs per SM, which sets the register budget.  Three CTAs
-// (80 registers) suit the one- and two-temperature kernels: on the 16^3 diamond
-// workload the FP32 contraction runs 1.21x and the FP64 one 1.01x faster than
-// with two.  Four or more temperatures keep two CTAs, where three would spill.
-template <int KIND, int NT>
+// (80 registers) suit the FP32 contraction of one or two temperatures (1.21x
+// faster than two CTAs on the 16^3 diamond workload) and the counting kernel.
+// The FP64 contraction keeps two CTAs (128 registers): at 80 it spills, and the
+// spill traffic cancels the extra warps.
+template <int KIND, int NT, bool MIXED>
 constexpr int ctas_per_sm() {
-    return (KIND != 0 && NT >= 4) ? 2 : 3;
+    return (KIND == 0 || (MIXED && NT <= 2)) ? 3 : 2;
 }
 
 template <bool MIXED>
@@ -65,17 +66,24 @@ struct CT<true> {
 
 struct Layout {
     size_t z, kap, pt, sval, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, misc, total;
+    int allz;  // 1: the reciprocal cluster tables of all (i,j) at once, 0: one branch i at a time
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-__host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum) {
+// Shared memory per CTA below which the tables of all branches are kept at once
+// (three CTAs per SM still fit).
+constexpr size_t kAllZCap = 72 * 1024;
+
+__host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
+                                              int allz) {
     Layout L;
+    L.allz = allz;
     const size_t cs = mixed ? 8 : 16;  // complex size
     const size_t nb2 = (size_t)nb * nb;
     size_t o = 0;
     L.z = o;
-    o = al16(o + ((kind >= 2) ? (size_t)nb * npi * 9 * cs : 0));
+    o = al16(o + ((kind >= 2) ? (allz ? nb2 : (size_t)nb) * npi * 9 * cs : 0));
     L.kap = o;
     o = al16(o + ((kind >= 2) ? (size_t)ntri * 16 : 0));
     L.pt = o;
@@ -99,7 +107,7 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
     L.klt = o;
     o = al16(o + nb2 * 4);
     L.pre = o;
-    o = al16(o + (size_t)(kMaxNb + 1) * 4);
+    o = al16(o + (nb2 + 1) * 4);
     L.blk = o;  // non-empty atom-pair blocks of the class table: (first class, end, atom k, atom l)
     o = al16(o + (size_t)(kMaxNb / 3) * (kMaxNb / 3) * 16);
     L.seg = o;  // kind 3: first list position of each branch's q' segment, then the segments' prefix
@@ -108,6 +116,14 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
     o = al16(o + 8 * 4);
     L.total = o;
     return L;
+}
+
+__host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum) {
+    if (kind >= 2) {
+        Layout A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1);
+        if (A.total <= kAllZCap) return A;
+    }
+    return k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0);
 }
 
 template <bool MIXED>
@@ -121,6 +137,129 @@ __device__ __forceinline__ const float2* eig_table<true>(const DevSys& S) {
     return S.eigf;
 }
 
+// One entry of the reciprocal cluster table of branches (i, j):
+//   Z_p[s][r] = sum_{c in p} kappa_c sum_{u,t} Psi_c[u][t][s][r] e_i[u] e~'_j[t]
+__device__ __forceinline__ double2 k4_z_entry(const DevSys& S, const DevIfc& F, const double2* kap, int ch, int q0,
+                                              int ii, int i, int j, int pc, int sr) {
+    const int nb = S.nb;
+    const double2* ei = S.eig + (size_t)(q0 * nb + i) * nb;
+    const double2* ej = S.eig + (size_t)(ii * nb + j) * nb;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int x = F.cl_start[pc]; x < F.cl_start[pc + 1]; x++) {
+        const int c = F.cl_index[x];
+        const int4 at = F.atoms[c];
+        const double* ph = F.phi + (size_t)c * 81 + sr;
+        double2 t1 = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            const double2 eu = ei[3 * at.x + u];
+#pragma unroll
+            for (int t = 0; t < 3; t++) {
+                double2 et = ej[3 * at.y + t];
+                if (ch == 2) et = cconj(et);
+                const double2 pr = cmul(eu, et);
+                const double f = ph[(u * 3 + t) * 9];
+                t1.x = fma(f, pr.x, t1.x);
+                t1.y = fma(f, pr.y, t1.y);
+            }
+        }
+        acc = cmac(acc, kap[c], t1);
+    }
+    return acc;
+}
+
+// Contract one queued process of branches (i, j) against the table Zj and add
+// its weights for every temperature to accr/accw (LIST: also store its Gamma).
+template <int NT, bool MIXED, bool LIST>
+__device__ __forceinline__ void k4_entry(const P4Params& p, const typename CT<MIXED>::T* Zj,
+                                         const typename CT<MIXED>::T* PT, const int4* blkinfo, int nbk,
+                                         unsigned long long ent, double sigma, long long pos, int ch, int ii, int i,
+                                         int j, double omega, int m0, int m1, int m2, int n0, int n1, int n2,
+                                         double (&accr)[NT], double (&accw)[NT]) {
+    using C = CT<MIXED>;
+    using cx = typename C::T;
+    const DevSys& S = p.S;
+    const int nb = S.nb, nptk = S.nptk;
+    const int N0 = S.n[0], N1 = S.n[1], lsum = N0 + N1 + S.n[2];
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const double floor_sigma = (double)0.001f;
+    const bool neg = (ch != 0);  // class displacement D = m_k - m_l (++) or m_l - m_k (+-, --)
+    const cx* etab = eig_table<MIXED>(S);
+    const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;  // omega field of the (v,w) records
+    const int jj = (int)(ent >> 32), k = (int)((ent >> 8) & 0xff), l = (int)(ent & 0xff);
+    int a, b, c;
+    q_coords_t(S, jj, a, b, c);
+    int t0, t1, t2;
+    if (ch == 0) {
+        t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+    } else if (ch == 1) {
+        t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+    } else {
+        t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+    }
+    const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, S.n[2]));
+    const double w1 = wvw[4 * (ii * nb + j)];
+    const double w2 = wvw[4 * (jj * nb + k)];
+    const double w3 = wvw[4 * (ss * nb + l)];
+    const double sv = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
+    const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(sv, w2), -w3) : __dadd_rn(__dadd_rn(sv, -w2), -w3);
+    if (sigma <= floor_sigma) sigma = 1.0 / sqrtpi;
+    const double g = exp(-(delta * delta) / (sigma * sigma));
+    const double base = g / (sigma * sqrtpi * (omega * w1 * w2 * w3));
+    double v2 = 0.0;
+    if (LIST || !S.onlyharmonic) {
+        const cx* e2 = etab + (size_t)(jj * nb + k) * nb;
+        const cx* e3 = etab + (size_t)(ss * nb + l) * nb;
+        cx V = C::zero();
+        for (int bb = 0; bb < nbk; bb++) {
+            const int4 bi = blkinfo[bb];
+            const int p0 = bi.x, p1 = bi.y, a3 = bi.z, a4 = bi.w;
+            cx u[3], v[3];
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                u[x] = e2[3 * a3 + x];
+                if (ch != 0) u[x] = C::conj(u[x]);
+                v[x] = C::conj(e3[3 * a4 + x]);
+            }
+            for (int pc = p0; pc < p1; pc++) {
+                const cx* pt = PT + pc * lsum;
+                cx w = C::mul(C::mul(pt[a], pt[N0 + b]), pt[N0 + N1 + c]);
+                if (neg) w = C::conj(w);
+                const cx* z = Zj + pc * 9;
+                cx tt = C::zero();
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    cx h = C::zero();
+#pragma unroll
+                    for (int r = 0; r < 3; r++) h = C::mac(h, z[x * 3 + r], v[r]);
+                    tt = C::mac(tt, u[x], h);
+                }
+                V = C::mac(V, w, tt);
+            }
+        }
+        v2 = C::norm(V);
+    }
+    const size_t plane = (size_t)nptk * nb;
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        if (t < p.nT) {
+            const double* bz = p.bose + t * plane;
+            const double f1 = bz[ii * nb + j], f2 = bz[jj * nb + k], f3 = bz[ss * nb + l];
+            double bc;
+            if (ch == 0)
+                bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
+            else if (ch == 1)
+                bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
+            else
+                bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
+            const double wp4 = bc * base;
+            accr[t] = fma(wp4, v2, accr[t]);
+            accw[t] += wp4;
+            if (LIST) p.gamma_out[ch][pos] = wp4 * v2 * p.gamma_scale;
+        }
+    }
+}
+
 // Phase B: contract every queued process of the current work item, branch by branch.
 // LIST: also store each process's own Gamma at its list position (Ind_plusplus etc.).
 template <int NT, bool MIXED, bool LIST>
@@ -131,8 +270,7 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
     using cx = typename C::T;
     const DevSys& S = p.S;
     const DevIfc& F = p.F;
-    const int nb = S.nb, nb2 = nb * nb, npi = F.npi, nptk = S.nptk;
-    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2], lsum = N0 + N1 + N2;
+    const int nb = S.nb, nb2 = nb * nb, npi = F.npi;
     cx* Z = reinterpret_cast<cx*>(smem + L.z);
     const double2* kap = reinterpret_cast<const double2*>(smem + L.kap);
     const cx* PT = reinterpret_cast<const cx*>(smem + L.pt);
@@ -143,10 +281,7 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
     int* pre = reinterpret_cast<int*>(smem + L.pre);
     const int4* blkinfo = reinterpret_cast<const int4*>(smem + L.blk);
     const int nbk = reinterpret_cast<const int*>(smem + L.misc)[3];
-    const double sqrtpi = sqrt(3.141592653589793238);
-    const double floor_sigma = (double)0.001f;
-    const bool neg = (ch != 0);  // class displacement D = m_k - m_l (++) or m_l - m_k (+-, --)
-    const cx* etab = eig_table<MIXED>(S);
+    const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;
     for (int i = 0; i < nb; i++) {
         if (threadIdx.x == 0) {
             int acc = 0;
@@ -163,33 +298,9 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
             continue;
         }
         if (threadIdx.x == 0) atomicAdd(&p.stats[4], 1ull);
-        // reciprocal cluster table of branch i for every j
-        const double2* ei = S.eig + (size_t)(q0 * nb + i) * nb;
         for (int idx = threadIdx.x; idx < nb * npi * 9; idx += blockDim.x) {
             const int j = idx / (npi * 9), rem = idx - j * (npi * 9), pc = rem / 9, sr = rem - pc * 9;
-            const double2* ej = S.eig + (size_t)(ii * nb + j) * nb;
-            double2 acc = make_double2(0.0, 0.0);
-            for (int x = F.cl_start[pc]; x < F.cl_start[pc + 1]; x++) {
-                const int c = F.cl_index[x];
-                const int4 at = F.atoms[c];
-                const double* ph = F.phi + (size_t)c * 81 + sr;
-                double2 t1 = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int u = 0; u < 3; u++) {
-                    const double2 eu = ei[3 * at.x + u];
-#pragma unroll
-                    for (int t = 0; t < 3; t++) {
-                        double2 et = ej[3 * at.y + t];
-                        if (ch == 2) et = cconj(et);
-                        const double2 pr = cmul(eu, et);
-                        const double f = ph[(u * 3 + t) * 9];
-                        t1.x = fma(f, pr.x, t1.x);
-                        t1.y = fma(f, pr.y, t1.y);
-                    }
-                }
-                acc = cmac(acc, kap[c], t1);
-            }
-            Z[idx] = C::from(acc);
+            Z[idx] = C::from(k4_z_entry(S, F, kap, ch, q0, ii, i, j, pc, sr));
         }
         __syncthreads();
         // plain per-thread partial sums (a few tens of terms each); the cross-work-item
@@ -200,88 +311,14 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
             accr[t] = 0.0;
             accw[t] = 0.0;
         }
-        const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;  // omega field of the (v,w) records
         const double omega = wvw[4 * (q0 * nb + i)];
         for (int e = threadIdx.x; e < tot; e += blockDim.x) {
             int j = 0;
             while (j + 1 < nb && pre[j + 1] <= e) j++;
             const size_t qi = (size_t)(i * nb + j) * p.subcap + (e - pre[j]);
-            const unsigned long long ent = qbase[qi];
-            double sigma = qsig[qi];
-            const int jj = (int)(ent >> 32), k = (int)((ent >> 8) & 0xff), l = (int)(ent & 0xff);
-            int a, b, c;
-            q_coords_t(S, jj, a, b, c);
-            int t0, t1, t2;
-            if (ch == 0) {
-                t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
-            } else if (ch == 1) {
-                t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
-            } else {
-                t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
-            }
-            const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
-            const double w1 = wvw[4 * (ii * nb + j)];
-            const double w2 = wvw[4 * (jj * nb + k)];
-            const double w3 = wvw[4 * (ss * nb + l)];
-            const double s = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
-            const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2), -w3) : __dadd_rn(__dadd_rn(s, -w2), -w3);
-            if (sigma <= floor_sigma) sigma = 1.0 / sqrtpi;
-            const double g = exp(-(delta * delta) / (sigma * sigma));
-            const double base = g / (sigma * sqrtpi * (omega * w1 * w2 * w3));
-            double v2 = 0.0;
-            if (LIST || !S.onlyharmonic) {
-                const cx* Zj = Z + (size_t)j * npi * 9;
-                const cx* e2 = etab + (size_t)(jj * nb + k) * nb;
-                const cx* e3 = etab + (size_t)(ss * nb + l) * nb;
-                cx V = C::zero();
-                for (int bb = 0; bb < nbk; bb++) {
-                    const int4 bi = blkinfo[bb];
-                    const int p0 = bi.x, p1 = bi.y, a3 = bi.z, a4 = bi.w;
-                    cx u[3], v[3];
-#pragma unroll
-                    for (int x = 0; x < 3; x++) {
-                        u[x] = e2[3 * a3 + x];
-                        if (ch != 0) u[x] = C::conj(u[x]);
-                        v[x] = C::conj(e3[3 * a4 + x]);
-                    }
-                    for (int pc = p0; pc < p1; pc++) {
-                        const cx* pt = PT + pc * lsum;
-                        cx w = C::mul(C::mul(pt[a], pt[N0 + b]), pt[N0 + N1 + c]);
-                        if (neg) w = C::conj(w);
-                        const cx* z = Zj + pc * 9;
-                        cx tt = C::zero();
-#pragma unroll
-                        for (int x = 0; x < 3; x++) {
-                            cx h = C::zero();
-#pragma unroll
-                            for (int r = 0; r < 3; r++) h = C::mac(h, z[x * 3 + r], v[r]);
-                            tt = C::mac(tt, u[x], h);
-                        }
-                        V = C::mac(V, w, tt);
-                    }
-                }
-                v2 = C::norm(V);
-            }
+            k4_entry<NT, MIXED, LIST>(p, Z + (size_t)j * npi * 9, PT, blkinfo, nbk, qbase[qi], qsig[qi],
+                                      LIST ? qpos[qi] : 0, ch, ii, i, j, omega, m0, m1, m2, n0, n1, n2, accr, accw);
             my_contr++;
-            const size_t plane = (size_t)nptk * nb;
-#pragma unroll
-            for (int t = 0; t < NT; t++) {
-                if (t < p.nT) {
-                    const double* bz = p.bose + t * plane;
-                    const double f1 = bz[ii * nb + j], f2 = bz[jj * nb + k], f3 = bz[ss * nb + l];
-                    double bc;
-                    if (ch == 0)
-                        bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
-                    else if (ch == 1)
-                        bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
-                    else
-                        bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
-                    const double wp4 = bc * base;
-                    accr[t] = fma(wp4, v2, accr[t]);
-                    accw[t] += wp4;
-                    if (LIST) p.gamma_out[ch][qpos[qi]] = wp4 * v2 * p.gamma_scale;
-                }
-            }
         }
         double v[2 * NT];
 #pragma unroll
@@ -300,6 +337,111 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
     }
     for (int x = threadIdx.x; x < nb2; x += blockDim.x) cnt[x] = 0;
     __syncthreads();
+}
+
+// Phase B with the tables of all (i,j) in shared memory at once: one table build
+// and one pass over every queued process of the work item.  A thread's entries
+// run in (i,j) order; its sums for one branch go to shared memory when its
+// branch changes.
+template <int NT, bool MIXED, bool LIST>
+__device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Layout& L,
+                               const unsigned long long* qbase, const double* qsig, const long long* qpos, int ch,
+                               int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
+                               unsigned long long& my_contr) {
+    using C = CT<MIXED>;
+    using cx = typename C::T;
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const int nb = S.nb, nb2 = nb * nb, npi = F.npi;
+    cx* Z = reinterpret_cast<cx*>(smem + L.z);
+    const double2* kap = reinterpret_cast<const double2*>(smem + L.kap);
+    const cx* PT = reinterpret_cast<const cx*>(smem + L.pt);
+    double* racc = reinterpret_cast<double*>(smem + L.racc);
+    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* pre = reinterpret_cast<int*>(smem + L.pre);
+    const int4* blkinfo = reinterpret_cast<const int4*>(smem + L.blk);
+    const int nbk = reinterpret_cast<const int*>(smem + L.misc)[3];
+    const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;
+    if (threadIdx.x == 0) {
+        int acc = 0, built = 0;
+        for (int i = 0; i < nb; i++) {
+            int bi = 0;
+            for (int j = 0; j < nb; j++) {
+                pre[i * nb + j] = acc;
+                acc += cnt[i * nb + j];
+                bi += cnt[i * nb + j];
+            }
+            built += (bi > 0);
+        }
+        pre[nb2] = acc;
+        if (built) atomicAdd(&p.stats[4], (unsigned long long)built);
+    }
+    __syncthreads();
+    const int tot = pre[nb2];
+    if (tot > 0) {
+        for (int idx = threadIdx.x; idx < nb2 * npi * 9; idx += blockDim.x) {
+            const int bin = idx / (npi * 9);
+            if (cnt[bin] == 0) continue;
+            const int rem = idx - bin * (npi * 9), pc = rem / 9, sr = rem - pc * 9;
+            const int i = bin / nb, j = bin - i * nb;
+            Z[idx] = C::from(k4_z_entry(S, F, kap, ch, q0, ii, i, j, pc, sr));
+        }
+        __syncthreads();
+        double accr[NT], accw[NT];
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            accr[t] = 0.0;
+            accw[t] = 0.0;
+        }
+        int bin = 0, cur_i = -1;
+        double omega = 0.0;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            while (pre[bin + 1] <= e) bin++;
+            const int i = bin / nb, j = bin - i * nb;
+            if (i != cur_i) {
+                if (cur_i >= 0) {
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        if (t < p.nT) {
+                            atomicAdd(&racc[cur_i * NT + t], accr[t]);
+                            atomicAdd(&wacc[cur_i * NT + t], accw[t]);
+                        }
+                        accr[t] = 0.0;
+                        accw[t] = 0.0;
+                    }
+                }
+                cur_i = i;
+                omega = wvw[4 * (q0 * nb + i)];
+            }
+            const size_t qi = (size_t)bin * p.subcap + (e - pre[bin]);
+            k4_entry<NT, MIXED, LIST>(p, Z + (size_t)bin * npi * 9, PT, blkinfo, nbk, qbase[qi], qsig[qi],
+                                      LIST ? qpos[qi] : 0, ch, ii, i, j, omega, m0, m1, m2, n0, n1, n2, accr, accw);
+            my_contr++;
+        }
+        if (cur_i >= 0) {
+#pragma unroll
+            for (int t = 0; t < NT; t++)
+                if (t < p.nT) {
+                    atomicAdd(&racc[cur_i * NT + t], accr[t]);
+                    atomicAdd(&wacc[cur_i * NT + t], accw[t]);
+                }
+        }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nb2; x += blockDim.x) cnt[x] = 0;
+    __syncthreads();
+}
+
+template <int NT, bool MIXED, bool LIST>
+__device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem, const Layout& L,
+                                         const unsigned long long* qbase, const double* qsig, const long long* qpos,
+                                         int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
+                                         unsigned long long& my_contr) {
+    if (L.allz)
+        k4_phase_b_all<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+    else
+        k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
 }
 
 // True (for the whole CTA) when some (i,j) queue could overflow within the next
@@ -361,7 +503,7 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
     int iter = 0;
     for (long long base = 0; base < total; base += blockDim.x, iter++) {
         if ((iter % kCheckEvery) == 0 && queue_nearly_full(p, cnt, nb2, misc))
-            k4_phase_b<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+            k4_flush<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
         const long long e = base + threadIdx.x;
         if (e >= total) continue;
         int i = 0;
@@ -400,7 +542,7 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
         qpos[qi] = pos;
     }
     __syncthreads();
-    k4_phase_b<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+    k4_flush<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
 }
 
 // Per-thread work counters of one kernel, flushed into a P4Params::stats array.
@@ -550,7 +692,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         for (int base = 0; base < total; base += blockDim.x, iter++) {
             if (KIND == 2 && (iter % kCheckEvery) == 0) {
                 if (queue_nearly_full(p, cnt, nb2, misc))
-                    k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                    k4_flush<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                                 my_contr);
             }
             if (base + (int)threadIdx.x < total) {
@@ -620,7 +762,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         }
         if (KIND == 2) {
             __syncthreads();
-            k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+            k4_flush<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                         my_contr);
         }
     }
@@ -643,7 +785,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
 }
 
 template <int KIND, int NT, bool MIXED>
-__global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT>())) k4_work(P4Params p) {
+__global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT, MIXED>())) k4_work(P4Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int nb2 = p.S.nb * p.S.nb;
     const Layout L = k4_layout(KIND, NT, MIXED, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2]);
@@ -669,7 +811,7 @@ __global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT>())) k4_work(P
 // and rebuilds its per-CTA tables.  The queue is per CTA, sized for the largest
 // branch count the server admits.
 template <int NT, bool MIXED>
-__global__ void __launch_bounds__(kThreads, (ctas_per_sm<2, NT>())) k4_work_multi(const P4Params* slots, const K4Tick* tick,
+__global__ void __launch_bounds__(kThreads, (ctas_per_sm<2, NT, MIXED>())) k4_work_multi(const P4Params* slots, const K4Tick* tick,
                                                                                 int* counter, unsigned long long* queue,
                                                                                 double* queue_sigma, int cta_bins,
                                                                                 int subcap) {
@@ -766,10 +908,11 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
-int k4_ctas_per_sm(int kind, int nT) {
-    if (kind == 0) return ctas_per_sm<0, 1>();
+int k4_ctas_per_sm(int kind, int nT, bool mixed) {
+    if (kind == 0) return ctas_per_sm<0, 1, false>();
     const int NT = round_nt(nT);
-    return NT >= 4 ? ctas_per_sm<2, 4>() : ctas_per_sm<2, 1>();
+    if (mixed) return NT >= 4 ? ctas_per_sm<2, 4, true>() : ctas_per_sm<2, 1, true>();
+    return ctas_per_sm<2, 1, false>();
 }
 
 cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nblocks, cudaStream_t st) {

@@ -12,7 +12,9 @@ converged conductivity, calling the C-ABI for every hot step:
 * tau_zero, iteration0, TConduct, symmetrize_tensor, the Gauss-Seidel
   iteration loop (iteration, or iteration_4ph with four_phonon_iteration)
   with twonorm3x3 relative change < eps (1232-1307);
-  BTE.kappa, BTE.kappa_tensor, BTE.kappa_scalar, BTE.KappaTensorVsT_RTA/CONV.
+  BTE.kappa, BTE.kappa_tensor, BTE.kappa_scalar, BTE.KappaTensorVsT_RTA/CONV;
+* BTE.w_final and the cumulative kappa files of CumulativeTConduct and
+  CumulativeTConductOmega (1315-1404).
 
 Numbers are written in the reference's Fortran edit descriptors (E20.10,
 E14.5, F7.1, I9, I0), so the files read the same way.
@@ -30,9 +32,12 @@ from . import abi
 def fortran_e(x: float, w: int, d: int) -> str:
     """Fortran Ew.d: 0.ddddE+xx right-justified in w columns."""
     x = float(x)
-    if x == 0.0 or not math.isfinite(x):
-        s = f"0.{'0' * d}E+00" if x == 0.0 else str(x)
-        return s.rjust(w)
+    if math.isnan(x):
+        return "NaN".rjust(w)
+    if math.isinf(x):
+        return ("-Infinity" if x < 0 else "Infinity").rjust(w)
+    if x == 0.0:
+        return f"0.{'0' * d}E+00".rjust(w)
     sign = "-" if x < 0 else ""
     a = abs(x)
     e = math.floor(math.log10(a)) + 1
@@ -108,6 +113,34 @@ def symmetrize_tensor(s, t):
     for R in s.sym.crotations:
         acc += R @ t @ R.T
     return acc / s.sym.nsymm_rot
+
+
+def write_final(tdir, s, F, ctx, T, nticks=100):
+    """BTE.w_final and the cumulative kappa files (ShengBTE.f90:1315-1404)."""
+    Fq = np.asarray(F).reshape(3, s.nptk, s.nb)  # F_n(b,q,d) as [d][q][b]
+    lines = []
+    for i in range(s.nb):
+        for ll in range(s.nlist):
+            q = s.wedge.list[ll] - 1
+            v = s.velocity[q, i, :]
+            f = Fq[:, q, i]
+            w = s.energy[q, i]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                tau = np.float64(np.dot(f, v)) / (np.float64(np.dot(v, v)) * w)
+                inv = np.float64(1.0) / tau
+            lines.append(fortran_e(w, 20, 10) + fortran_e(inv, 20, 10))
+    _rows(os.path.join(tdir, "BTE.w_final"), lines)
+    for omega_mode, name in ((False, "BTE.cumulative_kappa_tensor"), (True, "BTE.cumulative_kappaVsOmega_tensor")):
+        ticks, res = ctx.cumulative_tconduct(s, F, T=T, nticks=nticks, omega_mode=omega_mode)
+        r = res.reshape(nticks, 3, 3, s.nb)  # [k][d2][d1][b]
+        tens, scal = [], []
+        for k in range(nticks):
+            tot = sum(symmetrize_tensor(s, r[k, :, :, b].T) for b in range(s.nb))
+            tens.append(fortran_e(ticks[k], 20, 10) + "".join(fortran_e(x, 20, 10) for x in tot.ravel(order="F")))
+            scal.append(fortran_e(ticks[k], 20, 10) + fortran_e(np.trace(tot) / 3.0, 20, 10))
+        _rows(os.path.join(tdir, name), tens)
+        if not omega_mode:
+            _rows(os.path.join(tdir, "BTE.cumulative_kappa_scalar"), scal)
 
 
 def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(np.float32(1e-5)),
@@ -195,6 +228,7 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
                 f403.write(f"{T:7.1f}" + "".join(fortran_e(x, 14, 5) for x in ktot.ravel(order="F")) + f"{it:6d}\n")
                 res["kappa_conv"] = ktot.copy()
                 res["iterations"] = it
+            write_final(tdir, s, F, ctx, T)
             _rows(os.path.join(tdir, "BTE.kappa"), kappa_lines)
             _rows(os.path.join(tdir, "BTE.kappa_tensor"), tensor_lines)
             _rows(os.path.join(tdir, "BTE.kappa_scalar"), scalar_lines)

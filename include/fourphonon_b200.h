@@ -239,6 +239,21 @@ int fp4_last_stats(const fp4_ctx *ctx, int64_t *n_processes, int64_t *n_contract
                    double *kernel_ms, int64_t *launches);
 
 /*
+ * Replace CumulativeTConduct (Src/conductivity.f90:64-97) and
+ * CumulativeTConductOmega (100-148): ticks(nticks) (mean free paths in nm,
+ * 10**(8(i-1)/(nticks-1)-2) in default REAL; or angular frequencies
+ * emin+(emax-emin)*i/nticks with emax*1.1) and results(nbands,3,3,nticks),
+ * the kappa of the modes whose mean free path (omega) lies below each tick.
+ * The reference's nticks is 100 (config.f90:133).
+ */
+int fp4_cumulative_tconduct(fp4_ctx *ctx, const fp4_globals *g, double V, const double *omega,
+                            const double *velocity, const double *f_n, int32_t nticks, double *ticks,
+                            double *results);
+int fp4_cumulative_tconduct_omega(fp4_ctx *ctx, const fp4_globals *g, double V, const double *omega,
+                                  const double *velocity, const double *f_n, int32_t nticks, double *ticks,
+                                  double *results);
+
+/*
  * Allocation-free form of fp4_np_driver_4ph, for callers that cannot
  * allocate device memory (a host whose device memory all comes from its own
  * pool, or code embedded in a process whose allocator it must not touch).

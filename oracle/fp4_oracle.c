@@ -851,6 +851,82 @@ void fp4o_tconduct(const fp4o_sys *s, double V, const double *F, double *kappa) 
     for (int x = 0; x < nb * 9; x++) kappa[x] = fac * kappa[x] / den;
 }
 
+/* Euclidean norm of a 3-vector by the scaled sum of squares of reference BLAS dnrm2. */
+static double nrm2_3(const double x[3]) {
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < 3; i++) {
+        if (x[i] != 0.0) {
+            double a = fabs(x[i]);
+            if (scale < a) {
+                ssq = 1.0 + ssq * (scale / a) * (scale / a);
+                scale = a;
+            } else {
+                ssq = ssq + (a / scale) * (a / scale);
+            }
+        }
+    }
+    return scale * sqrt(ssq);
+}
+
+/*
+ * conductivity.f90:64-97 CumulativeTConduct (omega_mode 0: thresholds on the
+ * mean free path, ticks 10**(8(i-1)/(nticks-1)-2) nm evaluated in default
+ * REAL as there) and 100-148 CumulativeTConductOmega (omega_mode 1:
+ * thresholds on omega, ticks emin+(emax-emin)*i/nticks with emax*1.1).
+ * results(nb,3,3,nticks): results[((k*3 + d2)*3 + d1)*nb + b].
+ */
+void fp4o_cumulative_tconduct(const fp4o_sys *s, double V, const double *F, int nticks, int omega_mode,
+                              double *ticks, double *results) {
+    const int nb = s->nb, nptk = s->nptk;
+    if (omega_mode == 0) {
+        for (int ii = 1; ii <= nticks; ii++)
+            ticks[ii - 1] = (double)powf(10.0f, 8.0f * ((float)ii - 1.0f) / ((float)nticks - 1.0f) - 2.0f);
+    } else {
+        double emin = 1.e10, emax = -1.e10;
+        for (int ii = 1; ii <= nptk; ii++)
+            for (int jj = 1; jj <= nb; jj++) {
+                emin = fmin(emin, E(s, ii, jj));
+                emax = fmax(emax, E(s, ii, jj));
+            }
+        emax = emax * 1.1;
+        for (int ii = 1; ii <= nticks; ii++) ticks[ii - 1] = emin + (emax - emin) * ii / nticks;
+    }
+    for (size_t x = 0; x < (size_t)nb * 9 * nticks; x++) results[x] = 0.0;
+    for (int jj = 1; jj <= nb; jj++)
+        for (int ii = 2; ii <= nptk; ii++) {
+            double v[3], f[3], tmp[3][3];
+            for (int d = 0; d < 3; d++) {
+                v[d] = Vel(s, ii, jj, d);
+                f[d] = F[((size_t)d * nptk + (ii - 1)) * nb + (jj - 1)];
+            }
+            for (int d1 = 0; d1 < 3; d1++)
+                for (int d2 = 0; d2 < 3; d2++) tmp[d1][d2] = v[d1] * f[d2];
+            double w = E(s, ii, jj);
+            double fbe = 1.0 / (exp(FP4O_HBAR * w / FP4O_KB / s->T) - 1.0);
+            double pre = fbe * (fbe + 1) * w;
+            for (int d1 = 0; d1 < 3; d1++)
+                for (int d2 = 0; d2 < 3; d2++) tmp[d1][d2] = pre * tmp[d1][d2];
+            double lambda;
+            if (omega_mode == 0) {
+                double dot = 0.0;
+                for (int d = 0; d < 3; d++) dot = dot + f[d] * v[d];
+                lambda = dot / ((w + 1e-12) * nrm2_3(v));
+            } else {
+                lambda = w;
+            }
+            for (int k = 0; k < nticks; k++)
+                if (ticks[k] > lambda)
+                    for (int d1 = 0; d1 < 3; d1++)
+                        for (int d2 = 0; d2 < 3; d2++) {
+                            size_t o = (((size_t)k * 3 + d2) * 3 + d1) * nb + (jj - 1);
+                            results[o] = results[o] + tmp[d1][d2];
+                        }
+        }
+    double fac = (double)1e21f * (FP4O_HBAR * FP4O_HBAR);
+    double den = FP4O_KB * s->T * s->T * V * nptk;
+    for (size_t x = 0; x < (size_t)nb * 9 * nticks; x++) results[x] = fac * results[x] / den;
+}
+
 /* config.f90:503-518 symmetrize_tensor; crot(3,3,nsymm_rot) column-major. */
 void fp4o_symmetrize_tensor(int nsymm_rot, const double *crot, double *t /* t(3,3) col-major */) {
     double acc[9] = {0};

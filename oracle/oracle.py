@@ -244,6 +244,13 @@ class Oracle:
         lib().fp4o_tconduct(ct.byref(self.sys), ct.c_double(self.s.volume), _p(F), _p(k))
         return k
 
+    def cumulative_tconduct(self, F, nticks=100, omega_mode=False):
+        ticks = np.zeros(nticks)
+        res = np.zeros(self.s.nb * 9 * nticks)
+        lib().fp4o_cumulative_tconduct(ct.byref(self.sys), ct.c_double(self.s.volume), _p(F), nticks,
+                                       1 if omega_mode else 0, _p(ticks), _p(res))
+        return ticks, res
+
     def symmetrize_tensor(self, t33):
         crot = np.ascontiguousarray(np.transpose(self.s.sym.crotations, (0, 2, 1))).ravel()
         t = np.asfortranarray(t33).ravel(order="F").copy()
