@@ -96,8 +96,8 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     o = al16(o + (size_t)nb * NT * 8);
     L.pacc = o;
     o = al16(o + (size_t)nb * 8);
-    L.red = o;
-    o = al16(o + 32 * 2 * NT * 8);
+    L.red = o;  // block_sum_vec of 2*NT values (phase B) or 4 (work counters)
+    o = al16(o + (size_t)32 * (2 * NT > 4 ? 2 * NT : 4) * 8);
     L.sidx = o;
     o = al16(o + nb2 * 4);
     L.cnt = o;
@@ -287,7 +287,7 @@ __device__ void k4_phase_b(const P4Params& p, unsigned char* smem, const Layout&
             int acc = 0;
             for (int j = 0; j < nb; j++) {
                 pre[j] = acc;
-                acc += cnt[i * nb + j];
+                acc += min(cnt[i * nb + j], p.subcap);
             }
             pre[nb] = acc;
         }
@@ -369,8 +369,9 @@ __device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Lay
             int bi = 0;
             for (int j = 0; j < nb; j++) {
                 pre[i * nb + j] = acc;
-                acc += cnt[i * nb + j];
-                bi += cnt[i * nb + j];
+                const int n = min(cnt[i * nb + j], p.subcap);
+                acc += n;
+                bi += n;
             }
             built += (bi > 0);
         }
@@ -445,8 +446,12 @@ __device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem,
 }
 
 // True (for the whole CTA) when some (i,j) queue could overflow within the next
-// kCheckEvery passes of at most one new entry per thread.
+// kCheckEvery passes of at most one new entry per thread.  The barrier first
+// makes every thread's earlier appends visible: between checks the warps of the
+// CTA drift apart by up to kCheckEvery passes, so without it the counts read
+// here could be short by that many passes and a queue could overflow.
 __device__ __forceinline__ bool queue_nearly_full(const P4Params& p, const int* cnt, int nb2, int* misc) {
+    __syncthreads();
     if (threadIdx.x == 0) {
         int mx = 0;
         for (int b = 0; b < nb2; b++) mx = max(mx, cnt[b]);
@@ -536,6 +541,10 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
         if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0, Gamma = 0 (output pre-zeroed)
         const int idx = i * nb + j;
         const int qp = atomicAdd(&cnt[idx], 1);
+        if (qp >= p.subcap) {  // cannot happen with the capacity checks; never write past the bin
+            atomicOr(p.err, kErrQueue);
+            continue;
+        }
         const size_t qi = (size_t)idx * p.subcap + qp;
         qbase[qi] = pack4(jj, j, k, l);
         qsig[qi] = sigma_exact(S, w2, w3);
@@ -747,6 +756,10 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                             const double w1 = S.wv[ii * nb + j].w;
                             if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
                             const int pos = atomicAdd(&cnt[idx], 1);
+                            if (pos >= p.subcap) {  // cannot happen with the capacity checks
+                                atomicOr(p.err, kErrQueue);
+                                continue;
+                            }
                             qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
                             qsig[(size_t)idx * p.subcap + pos] = sigma;
                         }
