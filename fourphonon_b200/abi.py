@@ -285,6 +285,36 @@ class Context:
                                               *[_p(x) for x in lists], *[_p(d[k]) for k in names]))
         return d
 
+    def np_driver_4ph_sample(self, s, nsamples, seed):
+        """Sampled NP_driver_4ph: (N, P) per channel, as np_driver_4ph returns them."""
+        g = self.globals_of(s)
+        e, v, _, lst, ijk = self._arrays(s)
+        nm = s.nmodes
+        n = [np.zeros(nm, np.int64) for _ in range(3)]
+        p = [np.zeros(nm) for _ in range(3)]
+        self._chk(self.lib.fp4_np_driver_4ph_sample(self.h, ct.byref(g), _p(e), _p(v), s.nlist, _p(lst), _p(ijk),
+                                                    ct.c_int64(nsamples), ct.c_uint64(seed), _p(n[0]), _p(p[0]),
+                                                    _p(n[1]), _p(p[1]), _p(n[2]), _p(p[2])))
+        return n, p
+
+    def rta_driver_4ph_sample(self, s, nsamples, seed, temperatures=None):
+        """Sampled RTA_driver_4ph at each temperature; dict of (nT, nmodes) arrays."""
+        temps = np.ascontiguousarray(s.temperatures if temperatures is None else temperatures, dtype=np.float64)
+        g = self.globals_of(s, float(temps[0]))
+        e, v, z, lst, ijk = self._arrays(s)
+        f = self._ifc(s.ifc4)
+        nm = s.nmodes
+        nT = temps.size
+        out = [np.zeros(nm * nT) for _ in range(6)]
+        self._chk(self.lib.fp4_rta_driver_4ph_sample_multi_t(
+            self.h, ct.byref(g), nT, _p(temps), _p(e), _p(v), _p(z), s.nlist, _p(lst), _p(ijk), s.ifc4.ntri,
+            *[_p(x) for x in f], ct.c_int64(nsamples), ct.c_uint64(seed), *[_p(x) for x in out]))
+        names = ("rate_plusplus", "rate_plusminus", "rate_minusminus", "wp4_plusplus", "wp4_plusminus",
+                 "wp4_minusminus")
+        d = {k: o.reshape(nT, nm) for k, o in zip(names, out)}
+        d["rate_4ph"] = d["rate_plusplus"] + d["rate_plusminus"] + d["rate_minusminus"]
+        return d
+
     # -- BTE -------------------------------------------------------------------------
     def iteration0(self, s, tau_zero):
         g = self.globals_of(s)

@@ -239,6 +239,38 @@ int fp4_last_stats(const fp4_ctx *ctx, int64_t *n_processes, int64_t *n_contract
                    double *kernel_ms, int64_t *launches);
 
 /*
+ * Replace the sampled drivers: NP_driver_4ph with num_sample_process_4ph_phase_space
+ * > 0 (NP_plusplus_sample etc., Src/processes.f90:2480-2746) and RTA_driver_4ph
+ * with num_sample_process_4ph > 0 (RTA_plusplus_sample etc., 4811-5172):
+ * nsamples uniform draws of (q', j, q'', k, l) per mode and channel, scaled by
+ * nbands^3 nptk^2 / nsamples.  The reference draws from an unseeded
+ * random_number; here the draws come from a counter-based splitmix64 stream
+ * keyed by (seed, mode, channel, sample), so a (seed, nsamples) pair always
+ * gives the same estimate.  nsamples < 2^32.  The multi-temperature form
+ * weights the same samples for nT temperatures (outputs (nbands,nlist,nT)).
+ */
+int fp4_np_driver_4ph_sample(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                             int32_t nlist, const int32_t *list, const int32_t *ijk, int64_t nsamples,
+                             uint64_t seed, int64_t *n_plusplus, double *pspace_plusplus, int64_t *n_plusminus,
+                             double *pspace_plusminus, int64_t *n_minusminus, double *pspace_minusminus);
+int fp4_rta_driver_4ph_sample(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                              const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk,
+                              int32_t ntri, const double *psi, const double *r_j, const double *r_k,
+                              const double *r_l, const int32_t *index_i, const int32_t *index_j,
+                              const int32_t *index_k, const int32_t *index_l, int64_t nsamples, uint64_t seed,
+                              double *rate_4ph, double *rate_plusplus, double *rate_plusminus,
+                              double *rate_minusminus, double *wp4_plusplus, double *wp4_plusminus,
+                              double *wp4_minusminus);
+int fp4_rta_driver_4ph_sample_multi_t(fp4_ctx *ctx, const fp4_globals *g, int32_t nT, const double *temperatures,
+                                      const double *energy, const double *velocity, const double *eigenvect,
+                                      int32_t nlist, const int32_t *list, const int32_t *ijk, int32_t ntri,
+                                      const double *psi, const double *r_j, const double *r_k, const double *r_l,
+                                      const int32_t *index_i, const int32_t *index_j, const int32_t *index_k,
+                                      const int32_t *index_l, int64_t nsamples, uint64_t seed,
+                                      double *rate_plusplus, double *rate_plusminus, double *rate_minusminus,
+                                      double *wp4_plusplus, double *wp4_plusminus, double *wp4_minusminus);
+
+/*
  * Replace CumulativeTConduct (Src/conductivity.f90:64-97) and
  * CumulativeTConductOmega (100-148): ticks(nticks) (mean free paths in nm,
  * 10**(8(i-1)/(nticks-1)-2) in default REAL; or angular frequencies

@@ -700,6 +700,132 @@ int64_t fp4o_rta4_sample(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1,
 }
 
 /* ------------------------------------------------------------------------- */
+/* Sampled four-phonon estimators                                             */
+/* ------------------------------------------------------------------------- */
+
+/* splitmix64 finaliser (Steele, Lea and Flood, OOPSLA 2014). */
+static inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Key of sample n of mode mm (1-based) in channel ch: counter ((mm-1)*3+ch) << 32 | n. */
+uint64_t fp4o_sample_base(uint64_t seed, int mm, int ch, int64_t n) {
+    uint64_t c = ((uint64_t)((mm - 1) * 3 + ch) << 32) | (uint64_t)n;
+    return mix64(seed ^ mix64(c));
+}
+/* Draw k (0..4) of a sample, uniform on [0, range): high 64 bits of range * u. */
+static inline int draw_k(uint64_t base, int k, int range) {
+    uint64_t u = mix64(base + (uint64_t)k);
+    return (int)(((unsigned __int128)u * (uint64_t)range) >> 64);
+}
+
+/*
+ * NP_plusplus_sample ... / RTA_plusplus_sample ... (processes.f90:2480-2746,
+ * 4811-5172) for modes [mm0, mm1): nsamples uniform draws of (q', j, q'', k, l)
+ * per mode and channel, kept when inside the channel's restricted set
+ * (++: q''>=q', k>=j if q''=q'; +-: q'''>=q'', l>=k if q'''=q'', pair
+ * exclusions; --: both), weighted as the full drivers weight them and scaled by
+ * total_process/nsamples.  The draws come from the counter-based stream above
+ * in place of the reference's unseeded random_number, and exactly nsamples
+ * are drawn.  mode 0: counts and P4 (NP_*_sample); mode 2: Gamma and WP4
+ * (RTA_*_sample).  Output arrays are [ch][mode] (3 x nb*nlist).
+ */
+void fp4o_sample4(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int64_t nsamples, uint64_t seed,
+                  int mode, int64_t *n_out, double *p_out, double *rate_out, double *wp_out) {
+    const int nb = s->nb, nptk = s->nptk, nm = nb * s->nlist;
+    const int64_t total = (int64_t)nb * nptk * nb * nptk * nb;
+    const double hp = hbarp();
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+    for (int m0 = mm0; m0 < mm1; m0++)
+        for (int ch = 0; ch < 3; ch++) {
+            const int mm = m0 + 1;
+            const int i = (mm - 1) % nb + 1, ll = (mm - 1) / nb + 1;
+            int q[3];
+            for (int d = 0; d < 3; d++) q[d] = s->ijk[3 * (s->list[ll - 1] - 1) + d];
+            const double omega = E(s, s->list[ll - 1], i);
+            int64_t n = 0;
+            double P = 0.0, gamma = 0.0, wp = 0.0;
+            if (gate(s, mm) && omega != 0) {
+                for (int64_t it = 0; it < nsamples; it++) {
+                    uint64_t base = fp4o_sample_base(seed, mm, ch, it);
+                    int ii = draw_k(base, 0, nptk) + 1, j = draw_k(base, 1, nb) + 1;
+                    int jj = draw_k(base, 2, nptk) + 1, k = draw_k(base, 3, nb) + 1;
+                    int l = draw_k(base, 4, nb) + 1;
+                    int qp[3], qdp[3], qtp[3];
+                    for (int d = 0; d < 3; d++) {
+                        qp[d] = s->ijk[3 * (ii - 1) + d];
+                        qdp[d] = s->ijk[3 * (jj - 1) + d];
+                        int t = (ch == 0) ? (q[d] + qp[d] + qdp[d]) : (ch == 1) ? (q[d] + qp[d] - qdp[d])
+                                                                                 : (q[d] - qp[d] - qdp[d]);
+                        qtp[d] = fmodulo(t, s->ngrid[d]);
+                    }
+                    int ss = index_n(s, qtp);
+                    int accept;
+                    if (ch == 0)
+                        accept = jj >= ii && k >= ((jj == ii) ? j : 1);
+                    else if (ch == 1)
+                        accept = ss >= jj && l >= ((ss == jj) ? k : 1);
+                    else
+                        accept = jj >= ii && k >= ((jj == ii) ? j : 1) && ss >= jj && l >= ((ss == jj) ? k : 1);
+                    if (!accept) continue;
+                    double omegap = E(s, ii, j), omegadp = E(s, jj, k), omegatp = E(s, ss, l);
+                    if (!((omegap != 0) && (omegadp != 0) && (omegatp != 0))) continue;
+                    double sigma = sigma_of(s, jj, k, ss, l);
+                    if (ch == 1) {
+                        int ql = s->list[ll - 1];
+                        if (!((ql != jj || i != k) && (ql != ss || i != l) && (ii != jj || j != k) &&
+                              (ii != ss || j != l)))
+                            continue;
+                    }
+                    double delta = (ch == 0) ? (omega + omegap + omegadp - omegatp)
+                                   : (ch == 1) ? (omega + omegap - omegadp - omegatp)
+                                               : (omega - omegap - omegadp - omegatp);
+                    if (!(fabs(delta) <= sigma)) continue;
+                    if (sigma <= (double)0.001f) sigma = 1 / sqrt(FP4O_PI);
+                    n++;
+                    if (mode == 0) {
+                        P = P + exp(-(delta * delta) / (sigma * sigma)) /
+                                    (sigma * sqrt(FP4O_PI) * ((double)nptk * (double)nptk * (double)nptk) *
+                                     (double)(nb * nb * nb * nb));
+                        continue;
+                    }
+                    double f1 = fbe(s, omegap), f2 = fbe(s, omegadp), f3 = fbe(s, omegatp);
+                    double bose = (ch == 0)   ? (f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3)
+                                  : (ch == 1) ? (f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3)
+                                              : ((1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3);
+                    double wp4 = bose * exp(-(delta * delta) / (sigma * sigma)) / sigma / sqrt(FP4O_PI) /
+                                 (omega * omegap * omegadp * omegatp);
+                    if (omegap <= 1.25 || omegadp <= 1.25 || omegatp <= 1.25) wp4 = 0;
+                    wp = wp + wp4;
+                    if (!s->onlyharmonic) {
+                        double rqp[3], rqdp[3], rqtp[3], vr, vi;
+                        realq(s, qp, rqp);
+                        realq(s, qdp, rqdp);
+                        realq(s, qtp, rqtp);
+                        fp4o_vp4(s, f, ch, i, j, k, l, s->list[ll - 1], ii, jj, ss, rqp, rqdp, rqtp, &vr, &vi);
+                        double av = hypot(vr, vi);
+                        gamma = gamma + hp * hp * FP4O_PI / 8.0 * wp4 * (av * av);
+                    }
+                }
+                if (mode == 2) wp = wp / nptk / nptk;
+            }
+            const size_t o = (size_t)ch * nm + m0;
+            if (mode == 0) {
+                n_out[o] = (int64_t)((double)n / (double)nsamples * (double)total);
+                p_out[o] = P * (double)total / (double)nsamples;
+            } else {
+                gamma = gamma * (double)3.37617087f * 1.e9 / nptk / nptk;
+                rate_out[o] = gamma / (double)nsamples * (double)total;
+                wp_out[o] = wp * (double)total / (double)nsamples;
+                if (n_out) n_out[o] = n;
+            }
+        }
+}
+
+/* ------------------------------------------------------------------------- */
 /* Iterative BTE and thermal conductivity                                     */
 /* ------------------------------------------------------------------------- */
 

@@ -244,6 +244,18 @@ class Oracle:
         lib().fp4o_tconduct(ct.byref(self.sys), ct.c_double(self.s.volume), _p(F), _p(k))
         return k
 
+    def sample4(self, nsamples, seed, mode=2, mm0=0, mm1=None):
+        """Seeded NP_*_sample (mode 0) / RTA_*_sample (mode 2): arrays [ch][mode]."""
+        nm = self.s.nmodes
+        mm1 = nm if mm1 is None else mm1
+        n = np.zeros(3 * nm, np.int64)
+        p = np.zeros(3 * nm)
+        r = np.zeros(3 * nm)
+        w = np.zeros(3 * nm)
+        lib().fp4o_sample4(ct.byref(self.sys), ct.byref(self.ifc4) if self.ifc4 is not None else None, mm0, mm1,
+                           ct.c_int64(nsamples), ct.c_uint64(seed), mode, _p(n), _p(p), _p(r), _p(w))
+        return dict(n=n.reshape(3, nm), p=p.reshape(3, nm), rate=r.reshape(3, nm), wp=w.reshape(3, nm))
+
     def cumulative_tconduct(self, F, nticks=100, omega_mode=False):
         ticks = np.zeros(nticks)
         res = np.zeros(self.s.nb * 9 * nticks)
