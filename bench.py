@@ -486,7 +486,7 @@ def run_ours(args):
 # ---------------------------------------------------------------------------- serving stream
 
 
-def run_serving(args):
+def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
     """A Poisson stream of random-cell 3ph+4ph RTA requests through the serving
     path (mixed precision, continuous batching), against the same cells
     solved one at a time through the plain FP64 drivers."""
@@ -498,11 +498,13 @@ def run_serving(args):
     ctx = abi.Context(0, abi.FP4_PREC_FP64)
     for s in pool[:2]:  # warm-up (library load, first allocations)
         ctx.rta_driver(s, T=300.0)
-    k64, times = [], []
+    k64, times, nserial = [], [], 0
     for s in pool:
         t0 = time.perf_counter()
         r3 = ctx.rta_driver(s, T=300.0)
+        nserial += ctx.stats()[0]
         r4 = ctx.rta_driver_4ph(s, temperatures=[300.0])
+        nserial += ctx.stats()[0]
         rate = r3["rate_plus"] + r3["rate_minus"] + (r4["rate_plusplus"][0] + r4["rate_plusminus"][0]) + \
             r4["rate_minusminus"][0]
         tau = np.zeros_like(rate)
@@ -522,9 +524,12 @@ def run_serving(args):
     for i in range(len(pool), n):
         c = int(rng.integers(len(pool)))
         reqs.append(serve.Request(float(arrivals[i]), pool[c], float(rng.uniform(100.0, 1000.0)), tag=("rand", c)))
-    srv = serve.Server(0, abi.FP4_PREC_MIXED, max_slots=16, max_bands=12, hbm_budget=24 << 30)
-    tick_items = 32768
-    done, summ = serve.run_stream(srv, reqs, tick_items=tick_items)
+    precision = abi.FP4_PREC_MIXED if precision is None else precision
+    srv = serve.Server(0, precision, max_slots=max_slots, max_bands=12, hbm_budget=24 << 30)
+    # warm-up: every slot once through (allocates the slots' device buffers), untimed
+    warm = [serve.Request(0.0, pool[i % len(pool)], 300.0) for i in range(16)]
+    serve.run_stream(srv, warm, tick_items=1 << 16, target_tick_ms=tick_ms)
+    done, summ = serve.run_stream(srv, reqs, tick_items=1 << 16, target_tick_ms=tick_ms)
     srv.close()
     kerr = 0.0
     for r in done:
@@ -534,7 +539,10 @@ def run_serving(args):
     return {"requests": n, "solves_per_s": summ["solves_per_s"], "p50_ms": summ["p50_ms"], "p99_ms": summ["p99_ms"],
             "mean_ms": summ["mean_ms"], "processes_per_s": summ["processes_per_s"], "ticks": summ["ticks"],
             "serial_fp64_solves_per_s": 1.0 / t_serial, "vs_serial_fp64": summ["solves_per_s"] * t_serial,
-            "kappa_rel_err_max": kerr, "precision": "mixed", "max_slots": 16, "tick_items": tick_items,
+            "serial_fp64_processes_per_s": nserial / sum(times),
+            "kappa_rel_err_max": kerr, "precision": "mixed" if precision == abi.FP4_PREC_MIXED else "fp64",
+            "max_slots": max_slots, "tick_ms_target": tick_ms,
+            "host_s": summ["host_s"], "wall_s": summ["wall_s"],
             "arrivals": "Poisson at twice the serial FP64 rate",
             "workload": f"{len(pool)} random 2-4 atom cells (masses U[6,120] amu, seeded BvK + Gaussian IFCs), "
                         "grids 4^3-8^3 with nptk*nbands <= 3072, T~U[100,1000] K, 3ph+4ph RTA + kappa"}

@@ -133,6 +133,9 @@ __global__ void __launch_bounds__(256) k3_mode(P3Params p) {
         if (MODE != 1) qn += cnt;
         const bool last = (base + blockDim.x >= total);
         if (MODE != 1 && (qn > kQ3 - (int)blockDim.x || last)) {
+            // every thread's queue write of this pass must be visible before any thread
+            // reads the queue (the condition is uniform over the block)
+            __syncthreads();
             for (int e = threadIdx.x; e < qn; e += blockDim.x) {
                 const int xx = queue[e];
                 const int jj = xx / per_j, rem = xx - jj * per_j, q1 = rem / nb, kk = rem - q1 * nb;

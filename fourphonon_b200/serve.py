@@ -150,15 +150,22 @@ class Request:
         return self.finished - self.arrival
 
 
-def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_counter, sleep=time.sleep):
+def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_counter, sleep=time.sleep,
+               target_tick_ms=None, max_tick_items=1 << 22):
     """Serve `requests` (sorted by arrival) on the wall clock; returns them with
-    admission/finish times and results, plus a summary dict."""
+    admission/finish times and results, plus a summary dict.
+
+    With target_tick_ms, the number of work items per tick follows the last
+    tick's device time so that a tick lasts about that long: long enough to
+    hide the per-tick host work, short enough to admit new requests often."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     waiting = []
     running = {}
     nxt = 0
     t0 = clock()
     ticks = 0
+    items = int(tick_items)
+    t_admit = t_tick = t_collect = 0.0
     while nxt < len(reqs) or waiting or running:
         now = clock() - t0
         while nxt < len(reqs) and reqs[nxt].arrival <= now:
@@ -166,18 +173,29 @@ def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_cou
             nxt += 1
         while waiting:  # FIFO admission while slots and budget allow
             r = waiting[0]
+            ta = clock()
             slot = server.admit(r.solve, r.T)
+            t_admit += clock() - ta
             if slot is None:
                 break
             r.admitted = clock() - t0
             running[slot] = r
             waiting.pop(0)
         if running:
-            for slot in server.tick(tick_items):
+            tt = clock()
+            done = server.tick(items)
+            t_tick += clock() - tt
+            for slot in done:
                 r = running.pop(slot)
+                tc = clock()
                 r.result = server.collect(slot)
+                t_collect += clock() - tc
                 r.finished = clock() - t0
             ticks += 1
+            if target_tick_ms:
+                ms = server.status()["last_tick_ms"] if hasattr(server, "status") else 0.0
+                if ms > 0:
+                    items = int(min(max_tick_items, max(4096, items * target_tick_ms / ms)))
         elif nxt < len(reqs):
             sleep(max(0.0, reqs[nxt].arrival - (clock() - t0)))
     wall = clock() - t0
@@ -185,6 +203,7 @@ def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_cou
     summary = dict(requests=len(reqs), wall_s=wall, solves_per_s=len(reqs) / wall if wall > 0 else 0.0,
                    p50_ms=1e3 * float(np.percentile(lat, 50)), p99_ms=1e3 * float(np.percentile(lat, 99)),
                    mean_ms=1e3 * float(lat.mean()), ticks=ticks,
-                   processes=int(sum(r.result.get("n_processes", 0) for r in reqs)))
+                   processes=int(sum(r.result.get("n_processes", 0) for r in reqs)),
+                   host_s={"admit": t_admit, "tick": t_tick, "collect": t_collect})
     summary["processes_per_s"] = summary["processes"] / wall if wall > 0 else 0.0
     return reqs, summary
