@@ -535,7 +535,8 @@ def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
     for r in done:
         if r.tag[0] == "pool":
             ref = k64[r.tag[1]]
-            kerr = max(kerr, float(np.abs(r.result["kappa"] - ref).max() / np.abs(ref).max()))
+            if np.abs(ref).max() > 0:
+                kerr = max(kerr, float(np.abs(r.result["kappa"] - ref).max() / np.abs(ref).max()))
     return {"requests": n, "solves_per_s": summ["solves_per_s"], "p50_ms": summ["p50_ms"], "p99_ms": summ["p99_ms"],
             "mean_ms": summ["mean_ms"], "processes_per_s": summ["processes_per_s"], "ticks": summ["ticks"],
             "serial_fp64_solves_per_s": 1.0 / t_serial, "vs_serial_fp64": summ["solves_per_s"] * t_serial,

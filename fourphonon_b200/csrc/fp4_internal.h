@@ -84,6 +84,7 @@ cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nbloc
 size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F);
 int k4_threads();
 int k4_ctas_per_sm(int kind, int nT, bool mixed);
+int k4_multi_ctas_per_sm();
 cudaError_t launch_k4_multi(bool mixed, const P4Params* slots, const K4Tick* tick, int* counter,
                             unsigned long long* queue, double* queue_sigma, int cta_bins, int subcap, size_t smem,
                             int nblocks, cudaStream_t st);

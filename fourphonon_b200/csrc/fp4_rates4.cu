@@ -36,6 +36,10 @@ constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity che
 // faster than two CTAs on the 16^3 diamond workload) and the counting kernel.
 // The FP64 contraction keeps two CTAs (128 registers): at 80 it spills, and the
 // spill traffic cancels the extra warps.
+// The multi-solve kernel keeps more state per thread (the slot, its layout) and runs
+// two CTAs per SM in both precisions: at three the FP32 form spills.
+constexpr int kMultiCtasPerSm = 2;
+
 template <int KIND, int NT, bool MIXED>
 constexpr int ctas_per_sm() {
     return (KIND == 0 || (MIXED && NT <= 2)) ? 3 : 2;
@@ -395,10 +399,28 @@ __device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Lay
             accr[t] = 0.0;
             accw[t] = 0.0;
         }
-        int bin = 0, cur_i = -1;
+        // each thread loads its next queue entry one iteration ahead
+        int bin_n = 0, cur_i = -1;
         double omega = 0.0;
+        unsigned long long ent_n = 0;
+        double sig_n = 0.0;
+        if ((int)threadIdx.x < tot) {
+            while (pre[bin_n + 1] <= (int)threadIdx.x) bin_n++;
+            const size_t q1 = (size_t)bin_n * p.subcap + (threadIdx.x - pre[bin_n]);
+            ent_n = qbase[q1];
+            sig_n = qsig[q1];
+        }
         for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-            while (pre[bin + 1] <= e) bin++;
+            const int bin = bin_n;
+            const unsigned long long ent_c = ent_n;
+            const double sig_c = sig_n;
+            const int e2 = e + blockDim.x;
+            if (e2 < tot) {
+                while (pre[bin_n + 1] <= e2) bin_n++;
+                const size_t q2 = (size_t)bin_n * p.subcap + (e2 - pre[bin_n]);
+                ent_n = qbase[q2];
+                sig_n = qsig[q2];
+            }
             const int i = bin / nb, j = bin - i * nb;
             if (i != cur_i) {
                 if (cur_i >= 0) {
@@ -416,7 +438,7 @@ __device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Lay
                 omega = wvw[4 * (q0 * nb + i)];
             }
             const size_t qi = (size_t)bin * p.subcap + (e - pre[bin]);
-            k4_entry<NT, MIXED, LIST>(p, Z + (size_t)bin * npi * 9, PT, blkinfo, nbk, qbase[qi], qsig[qi],
+            k4_entry<NT, MIXED, LIST>(p, Z + (size_t)bin * npi * 9, PT, blkinfo, nbk, ent_c, sig_c,
                                       LIST ? qpos[qi] : 0, ch, ii, i, j, omega, m0, m1, m2, n0, n1, n2, accr, accw);
             my_contr++;
         }
@@ -824,7 +846,7 @@ __global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT, MIXED>())) k4
 // and rebuilds its per-CTA tables.  The queue is per CTA, sized for the largest
 // branch count the server admits.
 template <int NT, bool MIXED>
-__global__ void __launch_bounds__(kThreads, (ctas_per_sm<2, NT, MIXED>())) k4_work_multi(const P4Params* slots, const K4Tick* tick,
+__global__ void __launch_bounds__(kThreads, kMultiCtasPerSm) k4_work_multi(const P4Params* slots, const K4Tick* tick,
                                                                                 int* counter, unsigned long long* queue,
                                                                                 double* queue_sigma, int cta_bins,
                                                                                 int subcap) {
@@ -921,6 +943,8 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
+int k4_multi_ctas_per_sm() { return kMultiCtasPerSm; }
+
 int k4_ctas_per_sm(int kind, int nT, bool mixed) {
     if (kind == 0) return ctas_per_sm<0, 1, false>();
     const int NT = round_nt(nT);

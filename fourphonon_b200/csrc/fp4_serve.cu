@@ -34,7 +34,7 @@ int fp4_setup_ifc(fp4_ctx* c, const fp4_globals* g, int order, int32_t ntri, con
 
 namespace {
 
-constexpr size_t kSmemCap = 72 * 1024;  // dynamic shared memory of the multi-solve kernel (3 CTAs per SM)
+constexpr size_t kSmemCap = 72 * 1024;  // dynamic shared memory of the multi-solve kernel
 
 struct Slot {
     fp4_ctx* ctx = nullptr;
@@ -175,7 +175,7 @@ static int server_init(fp4_server* srv) {
     SCK(cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking));
     SCK(cudaEventCreate(&srv->e0));
     SCK(cudaEventCreate(&srv->e1));
-    srv->nblocks = srv->sm_count * k4_ctas_per_sm(2, 1, srv->precision == FP4_PREC_MIXED);
+    srv->nblocks = srv->sm_count * k4_multi_ctas_per_sm();
     srv->cta_bins = srv->max_bands * srv->max_bands;
     srv->subcap = 16 * k4_threads();
     const size_t qbytes = (size_t)srv->nblocks * srv->cta_bins * srv->subcap * (sizeof(unsigned long long) + sizeof(double));
