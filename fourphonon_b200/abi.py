@@ -13,6 +13,7 @@ subroutine writes into its intent(out) arguments, under the same names:
     ind_driver           -> Ind_driver         (processes.f90:524)
     iteration0/iteration -> iterations.f90:13 / 34
     tconduct             -> TConduct           (conductivity.f90:11)
+    eigen_dm             -> eigenDM / phonon_phonopy (phonon_routines.f90:12 / 84)
 
 The library is required: loading fails with an error if it is missing or was
 not built, and every failing call raises :class:`FP4Error` with the
@@ -378,6 +379,45 @@ class Context:
         symm = np.ascontiguousarray(np.transpose(s.sym.symmetrizers, (0, 2, 1))).ravel()
         self._chk(self.lib.fp4_symmetrize_fn(self.h, ct.byref(g), _p(symm), _p(F)))
         return F
+
+    def eigen_dm(self, cr, fc, ngrid, symmetrizers, born=None, epsilon=None, nonanalytic=False, V=None, rl=None):
+        """eigenDM on the device: omega (nptk,nb), velocity (nptk,nb,3) and
+        eigenvect (nptk,nb,nb) [q, band, component] for the crystal `cr`, the
+        read2fc array `fc` (natoms,3,sx,sy,sz,natoms,3) and symmetrizers
+        (nptk,3,3); with nonanalytic, the dielectric correction from born
+        (3,3,natoms) and epsilon (3,3). V and rl default to the crystal's
+        volume and reciprocal lattice."""
+        g = Globals()
+        for d in range(3):
+            g.ngrid[d] = int(ngrid[d])
+        nb = 3 * cr.natoms
+        g.nbands = nb
+        rl = cr.rlattvec() if rl is None else np.asarray(rl)
+        rlf = np.asfortranarray(rl).ravel(order="F")
+        for x in range(9):
+            g.rlattvec[x] = float(rlf[x])
+        masses = np.ascontiguousarray(cr.masses, dtype=np.float64)
+        types = np.ascontiguousarray(cr.types, dtype=np.int32)
+        self._keep = [masses, types]
+        g.nelements, g.natoms = masses.size, types.size
+        g.masses, g.types = _p(masses), _p(types)
+        nptk = int(np.prod(ngrid))
+        lv = np.asfortranarray(cr.lattvec, dtype=np.float64).ravel(order="F")
+        cart = np.asfortranarray(cr.cartesian, dtype=np.float64).ravel(order="F")
+        scell = np.array(cr.scell, dtype=np.int32)
+        fcf = np.asfortranarray(fc, dtype=np.float64).ravel(order="F")
+        symm = np.ascontiguousarray(np.transpose(symmetrizers, (0, 2, 1))).ravel()
+        eps = np.asfortranarray(np.eye(3) if epsilon is None else epsilon, dtype=np.float64).ravel(order="F")
+        bo = np.asfortranarray(np.zeros((3, 3, cr.natoms)) if born is None else born, dtype=np.float64).ravel(order="F")
+        vol = float(cr.volume() if V is None else V)
+        om = np.zeros(nptk * nb)
+        vel = np.zeros(nptk * nb * 3)
+        eig = np.zeros(nptk * nb * nb, dtype=np.complex128)
+        self._chk(self.lib.fp4_eigen_dm(self.h, ct.byref(g), _p(lv), _p(cart), _p(scell), _p(fcf),
+                                        int(bool(nonanalytic)), _p(eps), _p(bo), ct.c_double(vol), _p(symm), _p(om),
+                                        _p(vel), _p(eig)))
+        return (om.reshape((nptk, nb), order="F"), vel.reshape((nptk, nb, 3), order="F"),
+                eig.reshape((nptk, nb, nb), order="F"))
 
     def cumulative_tconduct(self, s, F, T=None, nticks=100, omega_mode=False):
         """CumulativeTConduct (or CumulativeTConductOmega): (ticks, results(nb,3,3,nticks) flat)."""

@@ -53,6 +53,7 @@ struct fp4_ctx {
     DevBuffer b_temps, b_bose, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
     DevBuffer b_queue, b_part, b_work, b_err, b_stats;
     DevBuffer b_bte[12];
+    DevBuffer b_harm[6];  // harmonic stage: pair ranges, terms, images, symmetrizers, outputs, born/masses
     IfcTables ifc3, ifc4;
     int64_t last_nproc = 0, last_ncontr = 0, last_launches = 0;
     int64_t last_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -66,6 +67,7 @@ struct fp4_ctx {
             v.push_back(&b_rootf[d]);
         }
         for (auto& b : b_bte) v.push_back(&b);
+        for (auto& b : b_harm) v.push_back(&b);
         for (auto* b : ifc3.list()) v.push_back(b);
         for (auto* b : ifc4.list()) v.push_back(b);
         return v;

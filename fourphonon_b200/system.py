@@ -120,18 +120,23 @@ def fc2_array(cr: C.Crystal, blocks: dict):
     return H.UNITFACTOR * fc
 
 
+def spring_fc(cr: C.Crystal, seed: int, spring_shells: int = 2, alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6)):
+    """The seeded BvK second-order constants of build_solve: (fc array of
+    read2fc, spring constants)."""
+    rng = np.random.default_rng(seed)
+    consts = [rng.uniform(*alpha_range)]
+    for s in range(1, spring_shells):
+        consts.append(rng.uniform(*beta_range) * (1.0 if s == 1 else 0.25))
+    return fc2_array(cr, G.bvk_fc2(cr, consts)), consts
+
+
 def build_solve(cr: C.Crystal, ngrid, temperatures, seed: int, fc3_shell: int = 3, fc4_shell: int = 1,
                 scalebroad: float = 1.0, with_4ph: bool = True, with_3ph: bool = True, spring_shells: int = 2,
                 alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6)) -> Solve:
     """Seeded synthetic solve: BvK springs (alpha per 1NN shell, beta per 2NN
     shell, further shells with beta/4), N(0,5) cubic and N(0,2) quartic
     clusters within the given neighbour-shell cutoffs."""
-    rng = np.random.default_rng(seed)
-    consts = [rng.uniform(*alpha_range)]
-    for s in range(1, spring_shells):
-        consts.append(rng.uniform(*beta_range) * (1.0 if s == 1 else 0.25))
-    blocks = G.bvk_fc2(cr, consts)
-    fc = fc2_array(cr, blocks)
+    fc, consts = spring_fc(cr, seed, spring_shells, alpha_range, beta_range)
     sym = C.build_symmetry(cr, ngrid)
     wd = C.wedge(sym)
     omega, vel, eig = H.eigen_dm(cr, fc, ngrid, sym.symmetrizers)

@@ -286,6 +286,26 @@ int fp4_cumulative_tconduct_omega(fp4_ctx *ctx, const fp4_globals *g, double V, 
                                   double *results);
 
 /*
+ * Replace eigenDM (Src/phonon_routines.f90:12-81) with phonon_phonopy
+ * (84-307) for a Phonopy FORCE_CONSTANTS_2ND without the dielectric
+ * correction when nonanalytic is set (lines 158-247): omega(nptk,nbands),
+ * velocity(nptk,nbands,3) and eigenvect(nptk,nbands,nbands) (complex,
+ * interleaved) on the Gamma-centred grid of g. lattvec(3,3) is in nm,
+ * cartesian(3,natoms) in nm, scell the supercell,
+ * fc(natoms,3,scell(1),scell(2),scell(3),natoms,3) the mass-reduced force
+ * constants of read2fc (Src/input.f90:18-79), epsilon(3,3) and
+ * born(3,3,natoms) the dielectric tensor and Born charges of CONTROL, V the
+ * cell volume in nm^3 and symmetrizers(3,3,nptk) those of symmetry_map.
+ * g->rlattvec gives the grid, g->masses and g->types the mass products.
+ * Eigenvectors carry LAPACK's freedom: an arbitrary phase per branch and an
+ * arbitrary basis inside a degenerate set.
+ */
+int fp4_eigen_dm(fp4_ctx *ctx, const fp4_globals *g, const double *lattvec, const double *cartesian,
+                 const int32_t scell[3], const double *fc, int32_t nonanalytic, const double *epsilon,
+                 const double *born, double V, const double *symmetrizers, double *omega, double *velocity,
+                 double *eigenvect);
+
+/*
  * Allocation-free form of fp4_np_driver_4ph, for callers that cannot
  * allocate device memory (a host whose device memory all comes from its own
  * pool, or code embedded in a process whose allocator it must not touch).

@@ -14,6 +14,11 @@ Example-Si) it stores, in ``<name>.npz``:
   (BTE.v_full), the wedge's List and Nequi (BTE.qpoints);
 * the lattice from CONTROL (rlattvec is recomputed from it in the
   reference's operation order, so the energy filter sees the same sigma);
+* where the example ships a Phonopy FORCE_CONSTANTS_2ND (LiCoO2, BAs), the
+  inputs of the harmonic stage: the read2fc array (mass-reduced, times
+  unitfactor), positions, types, scell, epsilon, born, the nonanalytic flag and
+  the element masses that data_calc_mandg (Src/data.f90:907-930) averages
+  from the isotope table of Src/data.f90;
 * the golden outputs of the counting stage: Ntotal_plus/minus and
   Ntotal_plusplus/plusminus/minusminus (log.out), per-mode four-phonon counts
   (BTE.Numprocess_4ph, whose line L holds the count of mode L), per-mode phase
@@ -33,6 +38,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 
+from fourphonon_b200 import harmonic as H  # noqa: E402
 from fourphonon_b200 import inputs as I  # noqa: E402
 
 
@@ -55,6 +61,23 @@ def rlattvec_ref(lattvec):
     V = abs(lattvec[0, 0] * r[0, 0] + lattvec[1, 0] * r[1, 0] + lattvec[2, 0] * r[2, 0])
     rV = 2.0 * np.pi / V
     return rV * r, V
+
+
+def element_masses(ref_root: str, elements):
+    """data_calc_mandg: the abundance-weighted mean of the isotope masses of
+    each element, in the table's order, divided by 100."""
+    txt = open(os.path.join(ref_root, "Src", "data.f90")).read()
+    el = {int(a): b for a, b in re.findall(r'isotope_element\((\d+)\)="(\w+)"', txt)}
+    ms = {int(a): float(b.replace("d", "e")) for a, b in re.findall(r"isotope_mass\((\d+)\)=([\d.d+-]+)", txt)}
+    ab = {int(a): float(b.replace("d", "e")) for a, b in re.findall(r"isotope_abundance\((\d+)\)=([\d.d+-]+)", txt)}
+    out = []
+    for e in elements:
+        m = 0.0
+        for i in sorted(el):
+            if el[i] == e:
+                m = m + ms[i] * ab[i]
+        out.append(m / 100.0)
+    return np.array(out)
 
 
 def build(ref_root: str, name: str):
@@ -95,6 +118,13 @@ def build(ref_root: str, name: str):
         f = os.path.join(out, "T300K", fn)
         if os.path.exists(f):
             d[key] = _floats(f).reshape(-1, 2)
+    fc2 = os.path.join(base, "input", "FORCE_CONSTANTS_2ND")
+    if os.path.exists(fc2):
+        cr = ctl.crystal()
+        cr.masses = element_masses(ref_root, ctl.elements)
+        d.update(fc2=H.read_fc2_phonopy(fc2, cr), masses=cr.masses, positions=ctl.positions,
+                 types=np.asarray(ctl.types, dtype=np.int32), scell=np.array(ctl.scell), epsilon=ctl.epsilon,
+                 born=ctl.born, nonanalytic=np.array(bool(ctl.flags["nonanalytic"])))
     np.savez_compressed(os.path.join(HERE, name.replace("Example-", "ref_") + ".npz"), **d)
     return d
 
