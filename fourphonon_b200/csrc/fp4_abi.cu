@@ -797,8 +797,9 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
         return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);
     int r;
     if ((r = c->b_temps.upload(c, temps, nT * sizeof(double)))) return r;
-    if ((r = c->b_bose.reserve(c, (size_t)S.nptk * S.nb * nT * sizeof(double)))) return r;
-    CK(launch_bose(S, c->b_temps.as<double>(), nT, c->b_bose.as<double>(), c->stream));
+    const int wbs = wb_stride(k4_round_nt(nT));
+    if ((r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wbs * sizeof(double)))) return r;
+    CK(launch_wbose(S, c->b_temps.as<double>(), nT, wbs, c->b_wb.as<double>(), c->stream));
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
     const int nblocks = k4_blocks(c, nwork, 2, nT);
@@ -811,7 +812,7 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     p.S = S;
     p.F = c->ifc4.F;
     p.nT = nT;
-    p.bose = c->b_bose.as<double>();
+    p.wb = c->b_wb.as<double>();
     p.nwork = nwork;
     p.work_counter = c->b_work.as<int>();
     p.part_rate = c->b_part.as<double>();
@@ -930,8 +931,8 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
         c->launches++;
     }
     if ((r = c->b_temps.upload(c, &g->T, sizeof(double)))) return r;
-    if ((r = c->b_bose.reserve(c, (size_t)S.nptk * S.nb * sizeof(double)))) return r;
-    CK(launch_bose(S, c->b_temps.as<double>(), 1, c->b_bose.as<double>(), c->stream));
+    if ((r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wb_stride(1) * sizeof(double)))) return r;
+    CK(launch_wbose(S, c->b_temps.as<double>(), 1, wb_stride(1), c->b_wb.as<double>(), c->stream));
     c->launches++;
     const int nwork = 3 * S.nlist * S.nptk;
     const int nblocks = k4_blocks(c, nwork, 3, 1);
@@ -943,7 +944,7 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
     p.S = S;
     p.F = c->ifc4.F;
     p.nT = 1;
-    p.bose = c->b_bose.as<double>();
+    p.wb = c->b_wb.as<double>();
     p.nwork = nwork;
     p.work_counter = c->b_work.as<int>();
     p.part_rate = c->b_part.as<double>();

@@ -50,7 +50,7 @@ struct fp4_ctx {
     std::vector<double> atom_mass;
     bool eig_packed = false;
     DevBuffer b_energy, b_velocity, b_wv, b_eigraw, b_eig, b_eigf, b_list, b_qc, b_root[3], b_rootf[3];
-    DevBuffer b_temps, b_bose, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
+    DevBuffer b_temps, b_bose, b_wb, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
     DevBuffer b_queue, b_part, b_work, b_err, b_stats;
     DevBuffer b_bte[12];
     DevBuffer b_harm[6];  // harmonic stage: pair ranges, terms, images, symmetrizers, outputs, born/masses
@@ -60,7 +60,7 @@ struct fp4_ctx {
     double last_ms = 0.0, last_kernel_ms = 0.0;
     std::vector<DevBuffer*> all_buffers() {
         std::vector<DevBuffer*> v = {&b_qc, &b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,
-                                     &b_temps,  &b_bose,     &b_out, &b_out4,   &b_lists, &b_gamma, &b_off,
+                                     &b_temps,  &b_bose,     &b_wb, &b_out, &b_out4,   &b_lists, &b_gamma, &b_off,
                                      &b_counts, &b_queue,    &b_part, &b_work,  &b_err,   &b_stats};
         for (int d = 0; d < 3; d++) {
             v.push_back(&b_root[d]);

@@ -251,9 +251,21 @@ __device__ __forceinline__ double bose_of(double w, double T) {
     return 1.0 / (exp(hbar * w / kb / T) - 1.0);
 }
 
-// 4-byte packed survivor (q'' index plus three branch indices) in a 64-bit word
-__device__ __forceinline__ unsigned long long pack4(int jj, int j, int k, int l) {
-    return ((unsigned long long)(unsigned)jj << 32) | ((unsigned)j << 16) | ((unsigned)k << 8) | (unsigned)l;
+// A queued four-phonon process in a 64-bit word: the grid coordinates (a,b,c) of
+// q'' (6 bits each, ngrid <= 64), the index of q''' (18 bits, nptk <= 64^3) and
+// the branches k, l (8 bits each).  j is the bin's.
+__device__ __forceinline__ unsigned long long pack_proc(int a, int b, int c, int ss, int k, int l) {
+    return ((unsigned long long)(unsigned)c << 46) | ((unsigned long long)(unsigned)b << 40) |
+           ((unsigned long long)(unsigned)a << 34) | ((unsigned long long)(unsigned)ss << 16) |
+           ((unsigned)k << 8) | (unsigned)l;
+}
+__device__ __forceinline__ void unpack_proc(unsigned long long e, int& a, int& b, int& c, int& ss, int& k, int& l) {
+    l = (int)(e & 0xff);
+    k = (int)((e >> 8) & 0xff);
+    ss = (int)((e >> 16) & 0x3ffff);
+    a = (int)((e >> 34) & 0x3f);
+    b = (int)((e >> 40) & 0x3f);
+    c = (int)((e >> 46) & 0x3f);
 }
 
 // Error flags raised by kernels (read back by the host after each call)

@@ -34,6 +34,7 @@ struct P4Params {
     DevIfc F;
     int nT;
     const double* bose;  // [t][q*nb+b]
+    const double* wb;    // [q*nb+b][wb_stride(NT)]: omega, the Bose factor at each T, padding
     int nwork;
     int* work_counter;
     int ch_of_work[3];
@@ -93,6 +94,11 @@ cudaError_t launch_k4_reduce(const P4Params& p, double* rate_pp, double* rate_pm
                              double* wp_pm, double* wp_mm, double rate_scale, cudaStream_t st);
 cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st);
 cudaError_t launch_bose(const DevSys& S, const double* T, int nT, double* bose, cudaStream_t st);
+// Per-mode records of the four-phonon contraction: omega and its Bose factors,
+// (NT + 1) doubles padded to an even count so that a record is whole 16-byte words.
+__host__ __device__ constexpr int wb_stride(int NT) { return (NT + 2) & ~1; }
+int k4_round_nt(int nT);  // the temperature count the four-phonon kernels are instantiated for (1, 2, 4, 8)
+cudaError_t launch_wbose(const DevSys& S, const double* T, int nT, int stride, double* wb, cudaStream_t st);
 cudaError_t prepare_k4_multi(bool mixed, size_t smem);
 // fp4_bte.cu: iteration0 and TConduct on device-resident arrays (reference layouts)
 cudaError_t launch_iteration0(int nb, int nptk, int nlist, int nsr, const int* nequi, const int* allequi,

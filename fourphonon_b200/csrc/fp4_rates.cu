@@ -331,6 +331,17 @@ __global__ void k_bose(DevSys S, const double* T, int nT, double* bose) {
     }
 }
 
+// omega and the Bose factors of every mode in one record per mode
+__global__ void k_wbose(DevSys S, const double* T, int nT, int stride, double* wb) {
+    const size_t plane = (size_t)S.nptk * S.nb;
+    for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < plane; m += (size_t)gridDim.x * blockDim.x) {
+        const double w = S.wv[m].w;
+        double* r = wb + m * stride;
+        r[0] = w;
+        for (int t = 1; t < stride; t++) r[t] = (t <= nT) ? bose_of(w, T[t - 1]) : 0.0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
@@ -360,6 +371,15 @@ cudaError_t launch_k3(int mode, const P3Params& p, int nmodes, cudaStream_t st) 
 
 cudaError_t launch_k4_order(const P4OrderParams& p, int nmodes, cudaStream_t st) {
     k4_order<<<nmodes, 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wbose(const DevSys& S, const double* T, int nT, int stride, double* wb, cudaStream_t st) {
+    if (nT + 1 > stride) return cudaErrorInvalidValue;
+    const size_t n = (size_t)S.nptk * S.nb;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    k_wbose<<<blocks, 256, 0, st>>>(S, T, nT, stride, wb);
     return cudaGetLastError();
 }
 

@@ -183,28 +183,22 @@ __device__ __forceinline__ void k4_entry(const P4Params& p, const typename CT<MI
     using C = CT<MIXED>;
     using cx = typename C::T;
     const DevSys& S = p.S;
-    const int nb = S.nb, nptk = S.nptk;
+    const int nb = S.nb;
     const int N0 = S.n[0], N1 = S.n[1], lsum = N0 + N1 + S.n[2];
     const double sqrtpi = sqrt(3.141592653589793238);
     const double floor_sigma = (double)0.001f;
     const bool neg = (ch != 0);  // class displacement D = m_k - m_l (++) or m_l - m_k (+-, --)
     const cx* etab = eig_table<MIXED>(S);
-    const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;  // omega field of the (v,w) records
-    const int jj = (int)(ent >> 32), k = (int)((ent >> 8) & 0xff), l = (int)(ent & 0xff);
-    int a, b, c;
-    q_coords_t(S, jj, a, b, c);
-    int t0, t1, t2;
-    if (ch == 0) {
-        t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
-    } else if (ch == 1) {
-        t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
-    } else {
-        t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
-    }
-    const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, S.n[2]));
-    const double w1 = wvw[4 * (ii * nb + j)];
-    const double w2 = wvw[4 * (jj * nb + k)];
-    const double w3 = wvw[4 * (ss * nb + l)];
+    int a, b, c, ss, k, l;
+    unpack_proc(ent, a, b, c, ss, k, l);
+    const int jj = q_index(S, a, b, c);
+    // (omega, Bose factors) records of the three other modes: omega now, the factors
+    // (same cache line) after the contraction, so that they are not live across it
+    constexpr int WS = wb_stride(NT);
+    const double* x1 = p.wb + (size_t)(ii * nb + j) * WS;
+    const double* x2 = p.wb + (size_t)(jj * nb + k) * WS;
+    const double* x3 = p.wb + (size_t)(ss * nb + l) * WS;
+    const double w1 = x1[0], w2 = x2[0], w3 = x3[0];
     const double sv = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
     const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(sv, w2), -w3) : __dadd_rn(__dadd_rn(sv, -w2), -w3);
     if (sigma <= floor_sigma) sigma = 1.0 / sqrtpi;
@@ -243,12 +237,10 @@ __device__ __forceinline__ void k4_entry(const P4Params& p, const typename CT<MI
         }
         v2 = C::norm(V);
     }
-    const size_t plane = (size_t)nptk * nb;
 #pragma unroll
     for (int t = 0; t < NT; t++) {
         if (t < p.nT) {
-            const double* bz = p.bose + t * plane;
-            const double f1 = bz[ii * nb + j], f2 = bz[jj * nb + k], f3 = bz[ss * nb + l];
+            const double f1 = x1[1 + t], f2 = x2[1 + t], f3 = x3[1 + t];
             double bc;
             if (ch == 0)
                 bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
@@ -539,8 +531,8 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
         const long long x2 = I2[pos] - 1, x3 = I3[pos] - 1, x4 = I4[pos] - 1;
         bool ok = x2 >= 0 && x2 < lim && x3 >= 0 && x3 < lim && x4 >= 0 && x4 < lim && x2 / nb == ii;
         const int j = (int)(x2 % nb), jj = (int)(x3 / nb), k = (int)(x3 % nb), ss = (int)(x4 / nb), l = (int)(x4 % nb);
+        int a = 0, b = 0, c = 0;
         if (ok) {
-            int a, b, c;
             q_coords_t(S, jj, a, b, c);
             int t0, t1, t2;
             if (ch == 0) {
@@ -568,7 +560,7 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
             continue;
         }
         const size_t qi = (size_t)idx * p.subcap + qp;
-        qbase[qi] = pack4(jj, j, k, l);
+        qbase[qi] = pack_proc(a, b, c, ss, k, l);
         qsig[qi] = sigma_exact(S, w2, w3);
         qpos[qi] = pos;
     }
@@ -782,7 +774,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                                 atomicOr(p.err, kErrQueue);
                                 continue;
                             }
-                            qbase[(size_t)idx * p.subcap + pos] = pack4(jj, j, k, l);
+                            qbase[(size_t)idx * p.subcap + pos] = pack_proc(a, b, c, ss, k, l);
                             qsig[(size_t)idx * p.subcap + pos] = sigma;
                         }
                     }
@@ -943,6 +935,7 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
+int k4_round_nt(int nT) { return round_nt(nT); }
 int k4_multi_ctas_per_sm() { return kMultiCtasPerSm; }
 
 int k4_ctas_per_sm(int kind, int nT, bool mixed) {

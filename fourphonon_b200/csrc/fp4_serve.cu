@@ -130,7 +130,7 @@ static int64_t footprint_of(int nb, int nlist, const int32_t ngrid[3], int ntri3
     const int64_t nptk = (int64_t)ngrid[0] * ngrid[1] * ngrid[2];
     const int64_t nm = (int64_t)nb * nlist;
     int64_t b = 0;
-    b += nptk * nb * (8 + 24 + 32 + 8);        // energy, velocity (raw and packed), Bose factors
+    b += nptk * nb * (8 + 24 + 32 + 8 + 16);   // energy, velocity (raw and packed), Bose factors, (omega, Bose) records
     b += nptk * nb * nb * (16 + 16 + 8);       // eigenvectors raw, packed FP64, packed FP32
     b += 3 * nlist * nptk * nb * 2 * 8;        // per-work-item partial sums
     b += (int64_t)ntri3 * (27 * 8 + 64) + (int64_t)ntri4 * (81 * 8 + 80);
@@ -294,19 +294,19 @@ extern "C" int fp4_server_admit(fp4_server* srv, const fp4_globals* g, const dou
     // Bose factors at T, partial sums, outputs
     const int nwork = 3 * nlist * S.nptk;
     if ((r = c->b_temps.upload(c, &g->T, sizeof(double))) ||
-        (r = c->b_bose.reserve(c, (size_t)S.nptk * S.nb * sizeof(double))) ||
+        (r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wb_stride(1) * sizeof(double))) ||
         (r = c->b_part.reserve(c, (size_t)nwork * S.nb * 2 * sizeof(double))) ||
         (r = c->b_out4.reserve(c, (size_t)nm * 6 * sizeof(double))) ||
         (r = c->b_out.reserve(c, (size_t)nm * 4 * sizeof(double) + (size_t)S.nb * 9 * sizeof(double))))
         return pass(r);
-    if (launch_bose(S, c->b_temps.as<double>(), 1, c->b_bose.as<double>(), c->stream) != cudaSuccess)
-        return sfail(srv, FP4_E_CUDA, "launch_bose failed");
+    if (launch_wbose(S, c->b_temps.as<double>(), 1, wb_stride(1), c->b_wb.as<double>(), c->stream) != cudaSuccess)
+        return sfail(srv, FP4_E_CUDA, "launch_wbose failed");
     P4Params& p = sl.p;
     p = P4Params{};
     p.S = S;
     p.F = c->ifc4.F;
     p.nT = 1;
-    p.bose = c->b_bose.as<double>();
+    p.wb = c->b_wb.as<double>();
     p.nwork = nwork;
     p.subcap = srv->subcap;
     p.part_rate = c->b_part.as<double>();
