@@ -196,16 +196,17 @@ struct Comp {
     __device__ __forceinline__ double val() const { return s + c; }
 };
 
-__device__ __forceinline__ int lower_bound_d(const double* a, int n, double x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < x)
-            lo = mid + 1;
-        else
-            hi = mid;
+// First index i with a[i] >= x in a sorted a[0..n-1], by a descent over powers of two
+// from the largest one <= n: the step count depends only on n, so the lanes of a warp
+// stay together.
+__device__ __forceinline__ int lower_bound_desc(const double* a, int n, double x) {
+    int i = 0;
+    if (n <= 0) return 0;
+    for (int step = 1 << (31 - __clz(n)); step > 0; step >>= 1) {
+        const int y = i + step;
+        if (y <= n && a[y - 1] < x) i = y;
     }
-    return lo;
+    return i;
 }
 
 // ---------------------------------------------------------------------------

@@ -672,7 +672,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         }
         if (ok) {
             sval[rank] = s;
-            sidx[rank] = idx;
+            sidx[rank] = (i << 16) | j;  // the pair itself: no division by nb in the window loop
         }
         if (idx == 0) misc[1] = nvalid;
         cnt[idx] = 0;
@@ -744,15 +744,16 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                         my_sig++;
                         const double cen = (ch == 0) ? (w3.w - w2.w) : (w2.w + w3.w);
                         const double tol = 1e-12 * (1.0 + fabs(w2.w) + fabs(w3.w) + smax + sigma);
-                        int x = lower_bound_d(sval, ns, cen - sigma - tol);
+                        int x = lower_bound_desc(sval, ns, cen - sigma - tol);
                         for (; x < ns && sval[x] <= cen + sigma + tol; x++) {
                             my_cand++;
                             const double s = sval[x];
                             const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w)
                                                            : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
                             if (!(fabs(delta) <= sigma)) continue;
-                            const int idx = sidx[x];
-                            const int i = idx / nb, j = idx - i * nb;
+                            const int ij = sidx[x];
+                            const int i = ij >> 16, j = ij & 0xffff;
+                            const int idx = i * nb + j;
                             if (ch != 1 && jj == ii && k < j) continue;
                             if (ch == 1 && !((q0 != jj || i != k) && (q0 != ss || i != l) && (ii != jj || j != k) &&
                                              (ii != ss || j != l)))
