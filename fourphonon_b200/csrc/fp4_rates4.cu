@@ -69,7 +69,7 @@ struct CT<true> {
 };
 
 struct Layout {
-    size_t z, kap, pt, sval, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, misc, total;
+    size_t z, kap, pt, sval, swj, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, misc, total;
     int allz;  // 1: the reciprocal cluster tables of all (i,j) at once, 0: one branch i at a time
 };
 
@@ -94,12 +94,17 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     o = al16(o + ((kind >= 2) ? (size_t)npi * lsum * cs : 0));
     L.sval = o;
     o = al16(o + nb2 * 8);
+    L.swj = o;  // omega'_j of each sorted pair
+    o = al16(o + nb2 * 8);
     L.racc = o;
     o = al16(o + (size_t)nb * NT * 8);
     L.wacc = o;
     o = al16(o + (size_t)nb * NT * 8);
+    // counting: one copy of the per-branch count and phase-space sum per warp, so that
+    // the shared-memory atomics of a survivor contend within its warp only
+    const size_t ncopy = (kind == 0) ? kThreads / 32 : 1;
     L.pacc = o;
-    o = al16(o + (size_t)nb * 8);
+    o = al16(o + (size_t)nb * ncopy * 8);
     L.red = o;  // block_sum_vec of 2*NT values (phase B) or 4 (work counters)
     o = al16(o + (size_t)32 * (2 * NT > 4 ? 2 * NT : 4) * 8);
     L.sidx = o;
@@ -107,7 +112,7 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     L.cnt = o;
     o = al16(o + nb2 * 4);
     L.ncnt = o;
-    o = al16(o + (size_t)nb * 4);
+    o = al16(o + (size_t)nb * ncopy * 4);
     L.klt = o;
     o = al16(o + nb2 * 4);
     L.pre = o;
@@ -632,6 +637,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
     const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2];
     double2* kap = reinterpret_cast<double2*>(smem + L.kap);
     double* sval = reinterpret_cast<double*>(smem + L.sval);
+    double* swj = reinterpret_cast<double*>(smem + L.swj);
     double* racc = reinterpret_cast<double*>(smem + L.racc);
     double* wacc = reinterpret_cast<double*>(smem + L.wacc);
     double* pacc = reinterpret_cast<double*>(smem + L.pacc);
@@ -672,12 +678,13 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         }
         if (ok) {
             sval[rank] = s;
+            swj[rank] = wj_;
             sidx[rank] = (i << 16) | j;  // the pair itself: no division by nb in the window loop
         }
         if (idx == 0) misc[1] = nvalid;
         cnt[idx] = 0;
     }
-    for (int x = threadIdx.x; x < nb; x += blockDim.x) {
+    for (int x = threadIdx.x; x < nb * (KIND == 0 ? kThreads / 32 : 1); x += blockDim.x) {
         ncnt[x] = 0;
         pacc[x] = 0.0;
     }
@@ -760,15 +767,16 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                                 continue;
                             my_surv++;
                             if (KIND == 0) {
-                                atomicAdd(&ncnt[i], 1);
                                 const double sg = (sigma <= floor_sigma) ? 1.0 / sqrtpi : sigma;
                                 const double pc = exp(-(delta * delta) / (sg * sg)) /
                                                   (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
                                                    (double)(nb * nb * nb * nb));
-                                atomicAdd(&pacc[i], pc);
+                                const int o = (threadIdx.x >> 5) * nb + i;
+                                atomicAdd(&ncnt[o], 1);
+                                atomicAdd(&pacc[o], pc);
                                 continue;
                             }
-                            const double w1 = S.wv[ii * nb + j].w;
+                            const double w1 = swj[x];
                             if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
                             const int pos = atomicAdd(&cnt[idx], 1);
                             if (pos >= p.subcap) {  // cannot happen with the capacity checks
@@ -797,8 +805,14 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
     __syncthreads();
     if (KIND == 0) {
         for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-            if (ncnt[i]) atomicAdd(&p.n_count[ch * S.nlist * nb + ll * nb + i], (unsigned long long)ncnt[i]);
-            if (pacc[i] != 0.0) atomicAdd(&p.p_sum[ch * S.nlist * nb + ll * nb + i], pacc[i]);
+            unsigned long long n = 0;
+            double ps = 0.0;
+            for (int w = 0; w < kThreads / 32; w++) {  // fixed order over the warp copies
+                n += (unsigned long long)ncnt[w * nb + i];
+                ps += pacc[w * nb + i];
+            }
+            if (n) atomicAdd(&p.n_count[ch * S.nlist * nb + ll * nb + i], n);
+            if (ps != 0.0) atomicAdd(&p.p_sum[ch * S.nlist * nb + ll * nb + i], ps);
         }
     } else {
         for (int idx = threadIdx.x; idx < nb * NT; idx += blockDim.x) {
