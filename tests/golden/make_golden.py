@@ -18,7 +18,8 @@ Example-Si) it stores, in ``<name>.npz``:
   inputs of the harmonic stage: the read2fc array (mass-reduced, times
   unitfactor), positions, types, scell, epsilon, born, the nonanalytic flag and
   the element masses that data_calc_mandg (Src/data.f90:907-930) averages
-  from the isotope table of Src/data.f90;
+  from the isotope table of Src/data.f90, and the FORCE_CONSTANTS_3RD clusters
+  as read3fc (Src/input.f90:102-141) stores them;
 * the golden outputs of the counting stage: Ntotal_plus/minus and
   Ntotal_plusplus/plusminus/minusminus (log.out), per-mode four-phonon counts
   (BTE.Numprocess_4ph, whose line L holds the count of mode L), per-mode phase
@@ -125,6 +126,9 @@ def build(ref_root: str, name: str):
         d.update(fc2=H.read_fc2_phonopy(fc2, cr), masses=cr.masses, positions=ctl.positions,
                  types=np.asarray(ctl.types, dtype=np.int32), scell=np.array(ctl.scell), epsilon=ctl.epsilon,
                  born=ctl.born, nonanalytic=np.array(bool(ctl.flags["nonanalytic"])))
+        # the third-order clusters as read3fc leaves them (lattice-rounded cells)
+        cl, _ = I.read_fc_anharmonic(os.path.join(base, "input", "FORCE_CONSTANTS_3RD"), ctl.lattvec, 3)
+        d.update(fc3_phi=cl.phi, fc3_cells=cl.cells.astype(np.int8), fc3_atoms=cl.atoms.astype(np.int8))
     np.savez_compressed(os.path.join(HERE, name.replace("Example-", "ref_") + ".npz"), **d)
     return d
 

@@ -8,6 +8,7 @@ import numpy as np
 
 from fourphonon_b200 import crystal as C
 from fourphonon_b200 import harmonic as HM
+from fourphonon_b200 import ifcgen as G
 from fourphonon_b200 import system as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -33,6 +34,58 @@ class GoldenHarmonic:
 
     def kwargs(self):
         return dict(born=self.born, epsilon=self.epsilon, nonanalytic=self.nonanalytic, V=self.V, rl=self.rl)
+
+    def ifc3(self):
+        """The example's FORCE_CONSTANTS_3RD as read3fc stores it."""
+        cl = G.Clusters(order=3, phi=self.z["fc3_phi"], cells=self.z["fc3_cells"].astype(np.int64),
+                        atoms=self.z["fc3_atoms"].astype(np.int32))
+        return S.IFC.from_clusters(cl, self.cr.lattvec)
+
+    def solve(self, omega, vel, eig, scalebroad=None):
+        """A rate solve on the example's grid, wedge and clusters with the given
+        harmonic arrays; T = 300 K as in the example's T300K outputs."""
+        sym = C.build_symmetry(self.cr, self.ngrid)
+        wd = C.wedge(sym)
+        sb = float(self.z["scalebroad"]) if scalebroad is None else scalebroad
+        return S.Solve(self.cr, self.ngrid, np.asfortranarray(omega), np.asfortranarray(vel), np.asfortranarray(eig),
+                       sym, wd, [300.0], scalebroad=sb, ifc3=self.ifc3())
+
+    def w3(self):
+        """BTE.w_3ph_plus, _minus and the total at 300 K as [ll, branch] arrays
+        (the files list branch-major: line (i-1)*Nlist+ll)."""
+        nb = self.z["energy"].shape[1]
+        nl = len(self.z["list"])
+        return tuple(self.z[k][:, 1].reshape(nb, nl).T for k in ("w3_plus", "w3_minus", "w3"))
+
+
+# The BAs example's outputs were produced with scalebroad = 1 (its CONTROL says 0.1):
+# its 3ph counts in log.out match at 1, not at 0.1.
+RUN_SCALEBROAD = {"BAs": 1.0}
+
+
+def check_w3(gh, omega, rate_plus, rate_minus, modes=None):
+    """Rates per irreducible point summed over each degenerate set (the basis inside a
+    set is LAPACK's choice; the sum is basis-free) against BTE.w_3ph*, all three
+    printed with 10 significant digits.  rate_* are [ll, branch]; modes limits the
+    check to the first `modes` irreducible points."""
+    gp, gm, g3 = gh.w3()
+    lst = gh.z["list"] - 1
+    nl = gp.shape[0] if modes is None else modes
+    scale = g3.max()
+    worst = 0.0
+    nsets = 0
+    for ll in range(nl):
+        w = omega[lst[ll]]
+        for (a, b) in degenerate_sets(np.sign(w) * w * w, 1e-9 * float(np.max(omega) ** 2)):
+            for mine, ref in ((rate_plus, gp), (rate_minus, gm), (rate_plus + rate_minus, g3)):
+                r = ref[ll, a:b].sum()
+                m = mine[ll, a:b].sum()
+                err = abs(m - r)
+                assert err <= 2e-9 * abs(r) + 1e-14 * scale, (ll, a, b, m, r)
+                if r > 1e-6 * scale:
+                    worst = max(worst, err / r)
+            nsets += 1
+    return worst, nsets
 
 
 def check_against_golden(gh, omega, vel):
