@@ -69,9 +69,14 @@ struct CT<true> {
 };
 
 struct Layout {
-    size_t z, kap, pt, sval, swj, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, misc, total;
+    size_t z, kap, pt, sval, swj, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, jjl, misc, total;
     int allz;  // 1: the reciprocal cluster tables of all (i,j) at once, 0: one branch i at a time
+    int njjl;  // capacity of the list of q'' that the channel's restriction keeps (0: no list)
 };
+
+// The +- and -- channels keep a q'' only when q''' >= q''; phase A then walks a list of
+// those q'' (16-bit indices, built per work item) instead of testing every q''.
+constexpr int kMaxJJList = 16384;
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
@@ -80,9 +85,10 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15
 constexpr size_t kAllZCap = 72 * 1024;
 
 __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
-                                              int allz) {
+                                              int allz, int njjl) {
     Layout L;
     L.allz = allz;
+    L.njjl = njjl;
     const size_t cs = mixed ? 8 : 16;  // complex size
     const size_t nb2 = (size_t)nb * nb;
     size_t o = 0;
@@ -121,18 +127,28 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     o = al16(o + (size_t)(kMaxNb / 3) * (kMaxNb / 3) * 16);
     L.seg = o;  // kind 3: first list position of each branch's q' segment, then the segments' prefix
     o = al16(o + (size_t)(2 * nb + 1) * 8);
+    L.jjl = o;
+    o = al16(o + (size_t)njjl * 2 + 32 * 4);  // the list, then per-warp counts of the compaction
     L.misc = o;
     o = al16(o + 8 * 4);
     L.total = o;
     return L;
 }
 
-__host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum) {
+// nptk_list: the grid size when the kernel may use the q'' list (0: never).  The list
+// is kept only where it costs no other choice: the all-branch tables come first.
+__host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
+                                            int nptk_list) {
+    const int nl = (kind == 0 || kind == 2) && nptk_list <= kMaxJJList ? nptk_list : 0;
     if (kind >= 2) {
-        Layout A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1);
+        Layout A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1, nl);
+        if (A.total <= kAllZCap) return A;
+        A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1, 0);
         if (A.total <= kAllZCap) return A;
     }
-    return k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0);
+    Layout B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, nl);
+    if (nl && B.total > kAllZCap) B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, 0);
+    return B;
 }
 
 template <bool MIXED>
@@ -590,6 +606,44 @@ __device__ __forceinline__ void k4_flush_stats(unsigned long long* stats, K4Stat
     st = K4Stats{0, 0, 0, 0};
 }
 
+// The q'' >= jj_lo (in order) whose q''' = q +- q' - q'' (channel ch) is >= q'': an
+// ordered block-wide compaction into list; returns the count (the same in every thread).
+__device__ int k4_jj_list(const DevSys& S, int ch, int jj_lo, int n0, int n1, int n2, int m0, int m1, int m2,
+                          unsigned short* list, int* wcnt) {
+    const int n = S.nptk - jj_lo;
+    const int chunk = (n + blockDim.x - 1) / blockDim.x;
+    const int x0 = min(n, (int)threadIdx.x * chunk), x1 = min(n, x0 + chunk);
+    auto keep = [&](int x) {
+        const int jj = jj_lo + x;
+        int a, b, c;
+        q_coords_t(S, jj, a, b, c);
+        const int t0 = (ch == 1) ? n0 + m0 - a : n0 - m0 - a;
+        const int t1 = (ch == 1) ? n1 + m1 - b : n1 - m1 - b;
+        const int t2 = (ch == 1) ? n2 + m2 - c : n2 - m2 - c;
+        return q_index(S, wrapN(t0, S.n[0]), wrapN(t1, S.n[1]), wrapN(t2, S.n[2])) >= jj;
+    };
+    int cnt = 0;
+    for (int x = x0; x < x1; x++) cnt += keep(x);
+    // exclusive prefix of the per-thread counts over the block, in thread order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wcnt[warp] = inc;
+    __syncthreads();
+    int off = inc - cnt, total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        if (w < warp) off += wcnt[w];
+        total += wcnt[w];
+    }
+    for (int x = x0; x < x1; x++)
+        if (keep(x)) list[off++] = (unsigned short)(jj_lo + x);
+    __syncthreads();
+    return total;
+}
+
 // Per-CTA tables of one solve: (k,l) decode table, non-empty class blocks and
 // per-class phase tables.
 template <int KIND, bool MIXED>
@@ -714,7 +768,14 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         double smax = 0.0;
         for (int x = 0; x < ns; x++) smax = fmax(smax, fabs(sval[x]));
         const int jj_lo = (ch == 1) ? 0 : ii;
-        const int total = (nptk - jj_lo) * nb2;
+        // the +- and -- channels walk only the q'' whose q''' is not smaller
+        const bool use_list = (ch != 0) && L.njjl >= nptk;
+        const unsigned short* jjl = reinterpret_cast<const unsigned short*>(smem + L.jjl);
+        const int nq = use_list ? k4_jj_list(S, ch, jj_lo, n0, n1, n2, m0, m1, m2,
+                                             reinterpret_cast<unsigned short*>(smem + L.jjl),
+                                             reinterpret_cast<int*>(smem + L.jjl + al16((size_t)L.njjl * 2)))
+                                : nptk - jj_lo;
+        const int total = nq * nb2;
         // thread t covers index base+t; keep (jj, kl) of it incrementally
         const int Bq = blockDim.x / nb2, Br = blockDim.x % nb2;
         int cj = threadIdx.x / nb2, ckl = threadIdx.x % nb2;
@@ -726,7 +787,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                                                 my_contr);
             }
             if (base + (int)threadIdx.x < total) {
-                const int jj = jj_lo + cj;
+                const int jj = use_list ? (int)jjl[cj] : jj_lo + cj;
                 const int kl = klt[ckl];
                 const int k = kl >> 8, l = kl & 0xff;
                 int a, b, c;
@@ -830,7 +891,7 @@ template <int KIND, int NT, bool MIXED>
 __global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT, MIXED>())) k4_work(P4Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int nb2 = p.S.nb * p.S.nb;
-    const Layout L = k4_layout(KIND, NT, MIXED, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2]);
+    const Layout L = k4_layout(KIND, NT, MIXED, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
     int* misc = reinterpret_cast<int*>(smem + L.misc);
     k4_cta_init<KIND, MIXED>(p, smem, L);
     unsigned long long* qbase = p.queue + (size_t)blockIdx.x * nb2 * p.subcap;
@@ -889,7 +950,7 @@ __global__ void __launch_bounds__(kThreads, kMultiCtasPerSm) k4_work_multi(const
             int* dst = reinterpret_cast<int*>(&sp);
             for (int x = threadIdx.x; x < (int)(sizeof(P4Params) / sizeof(int)); x += blockDim.x) dst[x] = src[x];
             __syncthreads();
-            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2]);
+            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2], 0);
             k4_cta_init<2, MIXED>(sp, smem, L);
             cur = slot;
         }
@@ -945,7 +1006,7 @@ cudaError_t launch_k4_t(const P4Params& p, int nblocks, cudaStream_t st) {
 }  // namespace
 
 size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
-    Layout L = k4_layout(kind, round_nt(nT), mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2]);
+    Layout L = k4_layout(kind, round_nt(nT), mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], S.nptk);
     return L.total;
 }
 
@@ -977,7 +1038,9 @@ cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nbloc
     return cudaErrorInvalidValue;
 }
 
-size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F) { return k4_smem(2, 1, mixed, S, F); }
+size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F) {
+    return k4_layout(2, 1, mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], 0).total;
+}
 
 cudaError_t prepare_k4_multi(bool mixed, size_t smem) {
     return mixed ? cudaFuncSetAttribute(k4_work_multi<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
