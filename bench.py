@@ -77,8 +77,8 @@ def workload(grid, rank=0):
 
 
 def ref_flops_per_process(s):
-    """The reference's per-process contraction work (SURVEY convention):
-    644*Ntri4 + 40 real flops (Vp_pp/pm/mm plus weights)."""
+    """The reference formulation's per-process work: 644*Ntri4 + 40 real flops
+    (the 81-term Vp_pp/pm/mm contraction per cluster plus the weights)."""
     return 644.0 * s.ifc4.ntri + 40.0
 
 
