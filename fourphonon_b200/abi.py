@@ -286,6 +286,30 @@ class Context:
                                               *[_p(x) for x in lists], *[_p(d[k]) for k in names]))
         return d
 
+    def np_driver_sample(self, s, nsamples, seed):
+        """Sampled NP_driver: (n_plus, n_minus, p_plus, p_minus), as np_driver returns them."""
+        g = self.globals_of(s)
+        e, v, _, lst, ijk = self._arrays(s)
+        nm = s.nmodes
+        n_p = np.zeros(nm, np.int32); n_m = np.zeros(nm, np.int32)
+        p_p = np.zeros(nm); p_m = np.zeros(nm)
+        self._chk(self.lib.fp4_np_driver_sample(self.h, ct.byref(g), _p(e), _p(v), s.nlist, _p(lst), _p(ijk),
+                                                ct.c_int64(nsamples), ct.c_uint64(seed), _p(n_p), _p(p_p), _p(n_m),
+                                                _p(p_m)))
+        return n_p, n_m, p_p, p_m
+
+    def rta_driver_sample(self, s, nsamples, seed, T=None):
+        """Sampled RTA_driver at T (default: the solve's first temperature)."""
+        g = self.globals_of(s, T)
+        e, v, z, lst, ijk = self._arrays(s)
+        f = self._ifc(s.ifc3)
+        nm = s.nmodes
+        out = [np.zeros(nm) for _ in range(5)]
+        self._chk(self.lib.fp4_rta_driver_sample(self.h, ct.byref(g), _p(e), _p(v), _p(z), s.nlist, _p(lst), _p(ijk),
+                                                 s.ifc3.ntri, *[_p(x) for x in f], ct.c_int64(nsamples),
+                                                 ct.c_uint64(seed), *[_p(x) for x in out]))
+        return dict(rate=out[0], rate_plus=out[1], rate_minus=out[2], wp3_plus=out[3], wp3_minus=out[4])
+
     def np_driver_4ph_sample(self, s, nsamples, seed):
         """Sampled NP_driver_4ph: (N, P) per channel, as np_driver_4ph returns them."""
         g = self.globals_of(s)

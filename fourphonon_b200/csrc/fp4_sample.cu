@@ -306,6 +306,173 @@ __global__ void k4_sample_reduce(PSParams p, double rate_scale, double* rate, do
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Sampled three-phonon estimators: NP_plus/minus_sample (processes.f90:828-979)
+// and RTA_plus/minus_sample (1474-1672).  One CTA per (mode, channel); its
+// threads take the mode's `nsamples` draws in turn.  A draw is one integer of
+// [0, nb*nptk*nb) decoded as the reference decodes rand_num: q' = r/(nb*nb),
+// branch j = (r/nb) % nb, branch k = r % nb; q'' follows from the channel.  The
+// 2-sigma test and the weights are the full drivers'; the sums are scaled by
+// nb*nptk*nb/nsamples in the reference's operation order.  The draws come from
+// the counter-based stream of the four-phonon estimators under keys of their
+// own, so the CPU oracle draws exactly the same samples.
+// ---------------------------------------------------------------------------
+struct P3SParams {
+    DevSys S;
+    DevIfc F;
+    const double* bose;  // [q*nb+b] at T (rates)
+    long long nsamples;
+    unsigned long long seed;
+    double scale;  // hbarp*pi/4
+    double unit;   // 5.60626442 (REAL) * 1e8
+    int32_t* n_out[2];
+    double* p_out[2];
+    double* rate[2];
+    double* wp[2];
+    unsigned long long* stats;
+};
+
+template <int MODE>  // 0: counts and P3, 2: rates and WP3
+__global__ void __launch_bounds__(256) k3_sample(P3SParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const int nb = S.nb, nptk = S.nptk;
+    const int N0 = S.n[0], N1 = S.n[1], N2 = S.n[2];
+    const int mm = blockIdx.x, w = blockIdx.y, sign = (w == 0) ? 1 : -1;
+    const int ll = mm / nb, i = mm % nb;
+    const int q0 = S.list0[ll];
+    int n0, n1, n2;
+    q_coords_t(S, q0, n0, n1, n2);
+    const double omega = S.wv[q0 * nb + i].w;
+    const bool gate = omega <= S.omega_max;
+    const bool need_v = (MODE == 2) && !S.onlyharmonic;
+    double2* Z = reinterpret_cast<double2*>(smem_raw);  // npi*9 (rates)
+    if (!(gate && omega != 0.0)) {
+        if (threadIdx.x == 0) {
+            if (MODE == 0) {
+                p.n_out[w][mm] = 0;
+                p.p_out[w][mm] = 0.0;
+            } else {
+                p.rate[w][mm] = 0.0;
+                p.wp[w][mm] = 0.0;
+            }
+        }
+        return;
+    }
+    if (need_v) {  // Z_p[s][r] = sum_{c in p} mu_c exp(-2 pi i n.m_k/N) sum_t Phi_c[t][s][r] e_i[t]
+        const double2* ei = S.eig + (size_t)(q0 * nb + i) * nb;
+        for (int idx = threadIdx.x; idx < F.npi * 9; idx += blockDim.x) {
+            const int pc = idx / 9, sr = idx % 9;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int x = F.cl_start[pc]; x < F.cl_start[pc + 1]; x++) {
+                const int c = F.cl_index[x];
+                const int4 at = F.atoms[c];
+                const int4 mk = F.mk[c];
+                double2 kap = lattice_phase(S, n0, n1, n2, -mk.x, -mk.y, -mk.z);
+                kap.x *= F.mu[c];
+                kap.y *= F.mu[c];
+                const double* ph = F.phi + (size_t)c * 27 + sr;
+                double2 t1 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int t = 0; t < 3; t++) {
+                    const double2 e = ei[3 * at.x + t];
+                    const double f = ph[t * 9];
+                    t1.x = fma(f, e.x, t1.x);
+                    t1.y = fma(f, e.y, t1.y);
+                }
+                acc = cmac(acc, kap, t1);
+            }
+            Z[idx] = acc;
+        }
+    }
+    __syncthreads();
+    const int total3 = nb * nptk * nb;
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const unsigned long long key = (unsigned long long)((1u << 30) + (unsigned)(mm * 2 + w)) << 32;
+    unsigned long long my_n = 0;
+    Comp accP = {0.0, 0.0}, accR = {0.0, 0.0}, accW = {0.0, 0.0};
+    for (long long it = threadIdx.x; it < p.nsamples; it += blockDim.x) {
+        const unsigned long long base = mix64(p.seed ^ mix64(key | (unsigned long long)it));
+        const int r = draw_k(base, 0, total3);
+        const int k = r % nb, nn = r / nb, j = nn % nb, ii = nn / nb;
+        int a, b, c;
+        q_coords_t(S, ii, a, b, c);
+        const int ss = q_index(S, wrapN(n0 + sign * a, N0), wrapN(n1 + sign * b, N1), wrapN(n2 + sign * c, N2));
+        const double4 wp = S.wv[ii * nb + j];
+        const double4 wd = S.wv[ss * nb + k];
+        if (!(wp.w != 0.0 && wd.w != 0.0)) continue;
+        const double sigma = sigma_exact(S, wp, wd);
+        const double delta = (sign > 0) ? __dadd_rn(__dadd_rn(omega, wp.w), -wd.w)
+                                        : __dadd_rn(__dadd_rn(omega, -wp.w), -wd.w);
+        if (!(fabs(delta) <= 2.0 * sigma)) continue;
+        my_n++;
+        const double g = exp(-(delta * delta) / (sigma * sigma));
+        if (MODE == 0) {
+            accP.add(g / (sigma * sqrtpi * (double)((long long)nptk * nptk) * (double)(nb * nb * nb)));
+            continue;
+        }
+        const double fp = p.bose[ii * nb + j], fd = p.bose[ss * nb + k];
+        const double bose = (sign > 0) ? (fp - fd) : (fp + fd + 1.0);
+        const double wp3 = bose * g / sigma / sqrtpi / (omega * wp.w * wd.w);
+        accW.add(wp3);
+        if (!need_v) continue;
+        double2 V = make_double2(0.0, 0.0);
+        const double2* e1 = S.eig + (size_t)(ii * nb + j) * nb;
+        const double2* e2 = S.eig + (size_t)(ss * nb + k) * nb;
+        for (int blk = 0; blk < F.nblk; blk++) {
+            const int p0 = F.blk_start[blk], p1 = F.blk_start[blk + 1];
+            if (p0 == p1) continue;
+            const int a2 = blk / S.natoms, a3 = blk - a2 * S.natoms;
+            double2 u[3], v[3];
+#pragma unroll
+            for (int s = 0; s < 3; s++) {
+                u[s] = e1[3 * a2 + s];
+                if (sign < 0) u[s] = cconj(u[s]);
+                v[s] = cconj(e2[3 * a3 + s]);
+            }
+            for (int pc = p0; pc < p1; pc++) {
+                const int4 D = F.pi_d[pc];
+                const double2 ph = lattice_phase(S, a, b, c, sign * D.x, sign * D.y, sign * D.z);
+                const double2* z = Z + pc * 9;
+                double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int s = 0; s < 3; s++) {
+                    double2 h = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) h = cmac(h, z[s * 3 + q], v[q]);
+                    t = cmac(t, u[s], h);
+                }
+                V = cmac(V, ph, t);
+            }
+        }
+        accR.add(p.scale * wp3 * (V.x * V.x + V.y * V.y));
+    }
+    const double n = block_sum((double)my_n, red);
+    const double ns = (double)p.nsamples;
+    if (MODE == 0) {
+        const double P = block_sum(accP.val(), red);
+        if (threadIdx.x == 0) {
+            p.n_out[w][mm] = (int32_t)(n / ns * nb * nptk * nb);
+            p.p_out[w][mm] = P * nb * nptk * nb / ns;
+        }
+    } else {
+        double W = block_sum(accW.val(), red);
+        double R = block_sum(accR.val(), red);
+        if (threadIdx.x == 0) {
+            W = (sign > 0) ? W / nptk : W * 5.e-1 / nptk;
+            p.wp[w][mm] = W * nb * nptk * nb / ns;
+            R = R * nb * nptk * nb / ns;
+            R = R * p.unit / (double)nptk;
+            p.rate[w][mm] = (sign > 0) ? R : R * 5.e-1;
+            atomicAdd(&p.stats[0], (unsigned long long)n);
+            if (need_v) atomicAdd(&p.stats[1], (unsigned long long)n);
+        }
+    }
+}
+
 }  // namespace
 
 #define CK(call)                                                                                      \
@@ -456,5 +623,110 @@ extern "C" int fp4_rta_driver_4ph_sample(fp4_ctx* c, const fp4_globals* g, const
     if (r) return r;
     const int nm = g->nbands * nlist;
     for (int m = 0; m < nm; m++) rate_4ph[m] = rate_pp[m] + rate_pm[m] + rate_mm[m];
+    return FP4_OK;
+}
+
+// Sampled three-phonon estimators on the context's current system.
+static int run_sample3(fp4_ctx* c, int mode, const fp4_globals* g, int64_t nsamples, uint64_t seed, P3SParams& p) {
+    if (nsamples < 1) return fp4_fail(c, FP4_E_ARG, "nsamples must be >=1");
+    if (nsamples >= ((int64_t)1 << 32)) return fp4_fail(c, FP4_E_ARG, "nsamples must be < 2^32");
+    const DevSys& S = c->S;
+    if ((int64_t)S.nb * S.nptk * S.nb >= ((int64_t)1 << 31))
+        return fp4_fail(c, FP4_E_CAPACITY, "nbands*nptk*nbands must be < 2^31");
+    p.S = S;
+    p.F = c->ifc3.F;
+    p.nsamples = nsamples;
+    p.seed = seed;
+    p.scale = 1.05457172647e-22 * (double)1e22f * 3.141592653589793238 / 4.0;
+    p.unit = (double)5.60626442f * 1.e8;
+    p.stats = c->b_stats.as<unsigned long long>();
+    size_t sm = 0;
+    if (mode == 2) {
+        int r;
+        if ((r = c->b_temps.upload(c, &g->T, sizeof(double)))) return r;
+        if ((r = c->b_bose.reserve(c, (size_t)S.nptk * S.nb * sizeof(double)))) return r;
+        CK(launch_bose(S, c->b_temps.as<double>(), 1, c->b_bose.as<double>(), c->stream));
+        c->launches++;
+        p.bose = c->b_bose.as<double>();
+        if (!S.onlyharmonic) sm = (size_t)p.F.npi * 9 * sizeof(double2);
+        if (sm > 227 * 1024) return fp4_fail(c, FP4_E_CAPACITY, "3ph cluster table needs %zu B of shared memory", sm);
+    }
+    const dim3 grid(S.nb * S.nlist, 2);
+    CK(cudaEventRecord(c->evk0, c->stream));
+    if (mode == 2) {
+        CK(cudaFuncSetAttribute(k3_sample<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k3_sample<2><<<grid, 256, sm, c->stream>>>(p);
+    } else {
+        k3_sample<0><<<grid, 256, 0, c->stream>>>(p);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->evk1, c->stream));
+    c->kernel_timed = true;
+    c->launches++;
+    return FP4_OK;
+}
+
+extern "C" int fp4_np_driver_sample(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
+                                    int32_t nlist, const int32_t* list, const int32_t* ijk, int64_t nsamples,
+                                    uint64_t seed, int32_t* n_plus, double* p_plus, int32_t* n_minus,
+                                    double* p_minus) {
+    if (!c) return FP4_E_ARG;
+    if (!n_plus || !p_plus || !n_minus || !p_minus) return fp4_fail(c, FP4_E_ARG, "null output");
+    int r;
+    if ((r = fp4_begin(c)) || (r = fp4_setup_system(c, g, energy, velocity, nullptr, nlist, list, ijk))) return r;
+    const int nm = c->S.nb * nlist;
+    if ((r = c->b_out.reserve(c, (size_t)nm * 4 * sizeof(double)))) return r;
+    double* d = c->b_out.as<double>();
+    P3SParams p{};
+    p.p_out[0] = d;
+    p.p_out[1] = d + nm;
+    p.n_out[0] = reinterpret_cast<int32_t*>(d + 2 * nm);
+    p.n_out[1] = p.n_out[0] + nm;
+    if ((r = run_sample3(c, 0, g, nsamples, seed, p))) return r;
+    std::vector<double> hp((size_t)2 * nm);
+    std::vector<int32_t> hn((size_t)2 * nm);
+    CK(cudaMemcpyAsync(hp.data(), d, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hn.data(), p.n_out[0], hn.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if ((r = fp4_end(c))) return r;
+    for (int m = 0; m < nm; m++) {
+        p_plus[m] = hp[m];
+        p_minus[m] = hp[nm + m];
+        n_plus[m] = hn[m];
+        n_minus[m] = hn[nm + m];
+    }
+    return FP4_OK;
+}
+
+extern "C" int fp4_rta_driver_sample(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
+                                     const double* eigenvect, int32_t nlist, const int32_t* list, const int32_t* ijk,
+                                     int32_t ntri, const double* phi, const double* r_j, const double* r_k,
+                                     const int32_t* index_i, const int32_t* index_j, const int32_t* index_k,
+                                     int64_t nsamples, uint64_t seed, double* rate, double* rate_plus,
+                                     double* rate_minus, double* wp3_plus, double* wp3_minus) {
+    if (!c) return FP4_E_ARG;
+    if (!rate || !rate_plus || !rate_minus || !wp3_plus || !wp3_minus) return fp4_fail(c, FP4_E_ARG, "null output");
+    if (!eigenvect) return fp4_fail(c, FP4_E_ARG, "null eigenvect");
+    int r;
+    if ((r = fp4_begin(c)) || (r = fp4_setup_system(c, g, energy, velocity, eigenvect, nlist, list, ijk))) return r;
+    if ((r = fp4_setup_ifc(c, g, 3, ntri, phi, r_j, r_k, nullptr, index_i, index_j, index_k, nullptr, c->ifc3))) return r;
+    const int nm = c->S.nb * nlist;
+    if ((r = c->b_out.reserve(c, (size_t)nm * 4 * sizeof(double)))) return r;
+    double* d = c->b_out.as<double>();
+    P3SParams p{};
+    p.rate[0] = d;
+    p.rate[1] = d + nm;
+    p.wp[0] = d + 2 * nm;
+    p.wp[1] = d + 3 * nm;
+    if ((r = run_sample3(c, 2, g, nsamples, seed, p))) return r;
+    std::vector<double> h((size_t)nm * 4);
+    CK(cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((r = fp4_end(c))) return r;
+    for (int m = 0; m < nm; m++) {
+        rate_plus[m] = h[m];
+        rate_minus[m] = h[nm + m];
+        wp3_plus[m] = h[2 * nm + m];
+        wp3_minus[m] = h[3 * nm + m];
+        rate[m] = rate_plus[m] + rate_minus[m];
+    }
     return FP4_OK;
 }

@@ -239,6 +239,26 @@ int fp4_last_stats(const fp4_ctx *ctx, int64_t *n_processes, int64_t *n_contract
                    double *kernel_ms, int64_t *launches);
 
 /*
+ * Replace the sampled three-phonon drivers: NP_driver with
+ * num_sample_process_3ph_phase_space > 0 (NP_plus_sample / NP_minus_sample,
+ * Src/processes.f90:828-979) and RTA_driver with num_sample_process_3ph > 0
+ * (RTA_plus_sample / RTA_minus_sample, 1474-1672, with the driver's x0.5 on the
+ * emission rate): nsamples uniform draws of (q', j, k) per mode and channel,
+ * scaled by nbands^2 nptk / nsamples.  The draws come from the same kind of
+ * seeded stream as the four-phonon estimators (keys of their own).
+ * nsamples < 2^32; nbands^2 nptk < 2^31.
+ */
+int fp4_np_driver_sample(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                         int32_t nlist, const int32_t *list, const int32_t *ijk, int64_t nsamples, uint64_t seed,
+                         int32_t *n_plus, double *pspace_plus, int32_t *n_minus, double *pspace_minus);
+int fp4_rta_driver_sample(fp4_ctx *ctx, const fp4_globals *g, const double *energy, const double *velocity,
+                          const double *eigenvect, int32_t nlist, const int32_t *list, const int32_t *ijk,
+                          int32_t ntri, const double *phi, const double *r_j, const double *r_k,
+                          const int32_t *index_i, const int32_t *index_j, const int32_t *index_k, int64_t nsamples,
+                          uint64_t seed, double *rate, double *rate_plus, double *rate_minus, double *wp3_plus,
+                          double *wp3_minus);
+
+/*
  * Replace the sampled drivers: NP_driver_4ph with num_sample_process_4ph_phase_space
  * > 0 (NP_plusplus_sample etc., Src/processes.f90:2480-2746) and RTA_driver_4ph
  * with num_sample_process_4ph > 0 (RTA_plusplus_sample etc., 4811-5172):

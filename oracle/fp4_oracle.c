@@ -825,6 +825,93 @@ void fp4o_sample4(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int64_
         }
 }
 
+/* Key of three-phonon sample n of mode mm (1-based) in channel ch (0: absorption,
+ * 1: emission): counter (2^30 + (mm-1)*2 + ch) << 32 | n, apart from the 4ph keys. */
+uint64_t fp4o_sample3_base(uint64_t seed, int mm, int ch, int64_t n) {
+    uint64_t c = ((uint64_t)((1u << 30) + (uint32_t)((mm - 1) * 2 + ch)) << 32) | (uint64_t)n;
+    return mix64(seed ^ mix64(c));
+}
+
+/*
+ * NP_plus_sample / NP_minus_sample (processes.f90:828-979) and RTA_plus_sample /
+ * RTA_minus_sample (1474-1672) with the driver's omega_max gate and x0.5 on the
+ * emission rate (1735-1760), for modes [mm0, mm1): per mode and channel,
+ * nsamples uniform draws of one integer of [1, Nb*nptk*Nb] decoded as the
+ * reference decodes rand_num (q' = ii, branches j and k), the q'' of the
+ * channel, the 2-sigma test, and the full drivers' weights, scaled by
+ * Nb*nptk*Nb/nsamples in the reference's operation order.  The draws come from
+ * the counter-based stream above in place of random_number.  mode 0: counts
+ * (int32, as N_plus is) and P3; mode 2: Gamma and WP3.  Outputs [ch][mode].
+ */
+void fp4o_sample3(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int64_t nsamples, uint64_t seed,
+                  int mode, int32_t *n_out, double *p_out, double *rate_out, double *wp_out) {
+    const int nb = s->nb, nptk = s->nptk, nm = nb * s->nlist;
+    const int total3 = nb * nptk * nb;
+    const double hp = hbarp();
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+    for (int m0 = mm0; m0 < mm1; m0++)
+        for (int ch = 0; ch < 2; ch++) {
+            const int mm = m0 + 1, which = ch == 0 ? +1 : -1;
+            const int i = (mm - 1) % nb + 1, ll = (mm - 1) / nb + 1;
+            int q[3];
+            for (int d = 0; d < 3; d++) q[d] = s->ijk[3 * (s->list[ll - 1] - 1) + d];
+            const double omega = E(s, s->list[ll - 1], i);
+            int64_t n = 0;
+            double P = 0.0, gamma = 0.0, wp = 0.0;
+            const int on = gate(s, mm);
+            if (on && omega != 0) {
+                for (int64_t it = 0; it < nsamples; it++) {
+                    const int rand_num = draw_k(fp4o_sample3_base(seed, mm, ch, it), 0, total3) + 1;
+                    const int nn = (rand_num - 1) / nb + 1;
+                    const int k = (rand_num - 1) % nb + 1;
+                    const int j = (nn - 1) % nb + 1;
+                    const int ii = (nn - 1) / nb + 1;
+                    int qp[3], qdp[3];
+                    for (int d = 0; d < 3; d++) {
+                        qp[d] = s->ijk[3 * (ii - 1) + d];
+                        qdp[d] = fmodulo(q[d] + which * qp[d], s->ngrid[d]);
+                    }
+                    const int ss = index_n(s, qdp);
+                    const double omegap = E(s, ii, j), omegadp = E(s, ss, k);
+                    if (!((omegap != 0) && (omegadp != 0))) continue;
+                    const double sigma = sigma_of(s, ii, j, ss, k);
+                    const double delta = (which > 0) ? (omega + omegap - omegadp) : (omega - omegap - omegadp);
+                    if (!(fabs(delta) <= 2.0 * sigma)) continue;
+                    n++;
+                    if (mode == 0) {
+                        P = P + exp(-(delta * delta) / (sigma * sigma)) /
+                                    (sigma * sqrt(FP4O_PI) * (double)(nptk * nptk) * (double)(nb * nb * nb));
+                        continue;
+                    }
+                    const double fbep = fbe(s, omegap), fbedp = fbe(s, omegadp);
+                    const double bose = (which > 0) ? (fbep - fbedp) : (fbep + fbedp + 1);
+                    const double wp3 = bose * exp(-(delta * delta) / (sigma * sigma)) / sigma / sqrt(FP4O_PI) /
+                                       (omega * omegap * omegadp);
+                    wp = wp + wp3;
+                    if (!s->onlyharmonic) {
+                        double rqp[3], rqdp[3], vr, vi;
+                        realq(s, qp, rqp);
+                        realq(s, qdp, rqdp);
+                        fp4o_vp3(s, f, which, i, j, k, s->list[ll - 1], ii, ss, rqp, rqdp, &vr, &vi);
+                        const double av = hypot(vr, vi);
+                        gamma = gamma + hp * FP4O_PI / 4.0 * wp3 * (av * av);
+                    }
+                }
+                if (mode == 2) wp = (which > 0) ? wp / nptk : wp * 5.e-1 / nptk;
+            }
+            const size_t o = (size_t)ch * nm + m0;
+            if (mode == 0) {
+                n_out[o] = on ? (int32_t)((double)n / (double)nsamples * nb * nptk * nb) : 0;
+                p_out[o] = on ? P * nb * nptk * nb / (double)nsamples : 0.0;
+            } else {
+                gamma = gamma * nb * nptk * nb / (double)nsamples;
+                gamma = gamma * (double)5.60626442f * 1.e8 / nptk;
+                rate_out[o] = on ? ((which > 0) ? gamma : gamma * 5.e-1) : 0.0;
+                wp_out[o] = on ? wp * nb * nptk * nb / (double)nsamples : 0.0;
+            }
+        }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Iterative BTE and thermal conductivity                                     */
 /* ------------------------------------------------------------------------- */

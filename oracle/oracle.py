@@ -256,6 +256,19 @@ class Oracle:
                            ct.c_int64(nsamples), ct.c_uint64(seed), mode, _p(n), _p(p), _p(r), _p(w))
         return dict(n=n.reshape(3, nm), p=p.reshape(3, nm), rate=r.reshape(3, nm), wp=w.reshape(3, nm))
 
+    def sample3(self, nsamples, seed, mode=2, mm0=0, mm1=None):
+        """Seeded NP_plus/minus_sample (mode 0) / RTA_plus/minus_sample (mode 2):
+        arrays [ch][mode], ch 0 absorption, 1 emission (rate with the driver's x0.5)."""
+        nm = self.s.nmodes
+        mm1 = nm if mm1 is None else mm1
+        n = np.zeros(2 * nm, np.int32)
+        p = np.zeros(2 * nm)
+        r = np.zeros(2 * nm)
+        w = np.zeros(2 * nm)
+        lib().fp4o_sample3(ct.byref(self.sys), ct.byref(self.ifc3) if self.ifc3 is not None else None, mm0, mm1,
+                           ct.c_int64(nsamples), ct.c_uint64(seed), mode, _p(n), _p(p), _p(r), _p(w))
+        return dict(n=n.reshape(2, nm), p=p.reshape(2, nm), rate=r.reshape(2, nm), wp=w.reshape(2, nm))
+
     def cumulative_tconduct(self, F, nticks=100, omega_mode=False):
         ticks = np.zeros(nticks)
         res = np.zeros(self.s.nb * 9 * nticks)
