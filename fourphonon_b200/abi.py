@@ -14,6 +14,8 @@ subroutine writes into its intent(out) arguments, under the same names:
     iteration0/iteration -> iterations.f90:13 / 34
     tconduct             -> TConduct           (conductivity.f90:11)
     eigen_dm             -> eigenDM / phonon_phonopy (phonon_routines.f90:12 / 84)
+    np_driver_sample / rta_driver_sample         -> NP_/RTA_plus/minus_sample (processes.f90:828 / 1474)
+    np_driver_4ph_sample / rta_driver_4ph_sample -> NP_/RTA_plusplus..._sample (processes.f90:2480 / 4811)
 
 The library is required: loading fails with an error if it is missing or was
 not built, and every failing call raises :class:`FP4Error` with the
