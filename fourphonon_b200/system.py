@@ -156,6 +156,38 @@ def build_solve(cr: C.Crystal, ngrid, temperatures, seed: int, fc3_shell: int = 
     return s
 
 
+def load_inputs(directory, ctx=None) -> Solve:
+    """A solve from a FourPhonon input directory: CONTROL, a Phonopy
+    FORCE_CONSTANTS_2ND, FORCE_CONSTANTS_3RD and, when four_phonon is set and the
+    file is there, FORCE_CONSTANTS_4TH (the readers of Src/config.f90 and
+    Src/input.f90).  The harmonic stage (eigenDM) runs on the device through
+    ctx.eigen_dm when a context is given, else in the numpy restatement.
+    CONTROL must list masses(:): the isotope table that autoisotopes averages
+    is not part of this package."""
+    path = lambda name: os.path.join(directory, name)  # noqa: E731
+    ctl = I.read_control(path("CONTROL"))
+    cr = ctl.crystal()
+    if not np.all(np.asarray(cr.masses) > 0):
+        raise I.InputError("CONTROL must give masses(:) (autoisotopes needs the isotope table)")
+    fc = H.read_fc2_phonopy(path("FORCE_CONSTANTS_2ND"), cr)
+    sym = C.build_symmetry(cr, ctl.ngrid)
+    wd = C.wedge(sym)
+    nac = bool(ctl.flags["nonanalytic"])
+    if ctx is not None:
+        omega, vel, eig = ctx.eigen_dm(cr, fc, ctl.ngrid, sym.symmetrizers, born=ctl.born, epsilon=ctl.epsilon,
+                                       nonanalytic=nac)
+    else:
+        omega, vel, eig = H.eigen_dm(cr, fc, ctl.ngrid, sym.symmetrizers, ctl.born, ctl.epsilon, nac)
+    cl3, _ = I.read_fc_anharmonic(path("FORCE_CONSTANTS_3RD"), cr.lattvec, 3)
+    ifc4 = None
+    if ctl.flags["four_phonon"] and os.path.exists(path("FORCE_CONSTANTS_4TH")):
+        cl4, _ = I.read_fc_anharmonic(path("FORCE_CONSTANTS_4TH"), cr.lattvec, 4)
+        ifc4 = IFC.from_clusters(cl4, cr.lattvec)
+    return Solve(cr, tuple(ctl.ngrid), np.asfortranarray(omega), np.asfortranarray(vel), np.asfortranarray(eig), sym,
+                 wd, list(ctl.temperatures()), scalebroad=ctl.scalebroad, omega_max=ctl.omega_max,
+                 ifc3=IFC.from_clusters(cl3, cr.lattvec), ifc4=ifc4, onlyharmonic=bool(ctl.flags["onlyharmonic"]))
+
+
 def diamond_solve(ngrid=(6, 6, 6), temperatures=(300.0,), seed=20240601, **kw) -> Solve:
     """2-atom diamond, fcc a=5.43 A, masses 28.085 (workload of the 6^3 and 16^3 cases)."""
     return build_solve(C.diamond(5.43, (28.085, 28.085)), ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, **kw)
