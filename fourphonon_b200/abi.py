@@ -263,6 +263,16 @@ class Context:
         d["rate_4ph"] = d["rate_plusplus"] + d["rate_plusminus"] + d["rate_minusminus"]
         return d
 
+    def rta4_partials(self, s, ll, ii0, ii1, t=0):
+        """The last rta_driver_4ph call's rates and WP4 of irreducible point ll
+        (0-based) at temperature index t from the q' in [ii0, ii1): arrays of
+        nbands per channel, keyed like rta_driver_4ph's result."""
+        out = [np.zeros(s.nb) for _ in range(6)]
+        self._chk(self.lib.fp4_rta4_partials(self.h, ll, ii0, ii1, t, *[_p(x) for x in out]))
+        names = ("rate_plusplus", "rate_plusminus", "rate_minusminus", "wp4_plusplus", "wp4_plusminus",
+                 "wp4_minusminus")
+        return dict(zip(names, out))
+
     def ind_driver_4ph(self, s, n_pp, n_pm, n_mm, T=None):
         """Ind_driver_4ph: the three channels' index lists and per-process Gamma,
         rates and WP4 per mode.  Keys follow the oracle's ind4(), so the result

@@ -29,14 +29,17 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if not force and not needs_build():
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
+    from concurrent.futures import ThreadPoolExecutor
+
+    objs = [os.path.join(CSRC, src.replace(".cu", ".o")) for src in SOURCES]
+    cmds = [[NVCC, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj] for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    # the translation units compile independently; the largest takes most of the time
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-ccbin", "/usr/bin/g++", "-o", LIB, *objs,
            "-lcudart"]
     subprocess.run(cmd, check=True)

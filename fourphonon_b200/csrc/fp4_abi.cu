@@ -824,6 +824,7 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     CK(cudaEventRecord(c->evk1, c->stream));
     c->kernel_timed = true;
     c->launches++;
+    c->last_rta4_nT = nT;
     double* o = c->b_out4.as<double>();
     const size_t blk = (size_t)nm * nT;
     const double rate_scale = hbarp() * hbarp() * kPi / 8.0 * (double)3.37617087f * 1.e9;
@@ -851,6 +852,47 @@ extern "C" int fp4_rta_driver_4ph_multi_t(fp4_ctx* c, const fp4_globals* g, int3
     double* outs[6] = {rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm};
     for (int x = 0; x < 6; x++) CK(cudaMemcpyAsync(outs[x], o + x * blk, blk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return fp4_end(c);
+}
+
+// Per-q' parts of the last four-phonon RTA call: the rates and WP4 of list point ll
+// (0-based) at temperature t from the processes whose second phonon q' lies in
+// [ii0, ii1), normalised as the full driver normalises them.  The per-work-item
+// partial sums stay on the device until the next four-phonon call.
+extern "C" int fp4_rta4_partials(fp4_ctx* c, int32_t ll, int32_t ii0, int32_t ii1, int32_t t, double* rate_pp,
+                                 double* rate_pm, double* rate_mm, double* wp_pp, double* wp_pm, double* wp_mm) {
+    if (!c) return FP4_E_ARG;
+    const DevSys& S = c->S;
+    const int nT = c->last_rta4_nT;
+    if (nT < 1) return fp4_fail(c, FP4_E_STATE, "no four-phonon RTA call to inspect");
+    if (ll < 0 || ll >= S.nlist || ii0 < 0 || ii1 > S.nptk || ii0 >= ii1 || t < 0 || t >= nT)
+        return fp4_fail(c, FP4_E_ARG, "partials: ll=%d q' [%d,%d) t=%d outside the last call", ll, ii0, ii1, t);
+    if (!rate_pp || !rate_pm || !rate_mm || !wp_pp || !wp_pm || !wp_mm) return fp4_fail(c, FP4_E_ARG, "null output");
+    const int nb = S.nb;
+    const size_t nwork = (size_t)3 * S.nlist * S.nptk;
+    const size_t per_q = (size_t)3 * nT * nb;  // the three channels' records of one q'
+    const size_t first = ((size_t)ll * S.nptk + ii0) * 3;
+    const size_t n = (size_t)(ii1 - ii0) * per_q;
+    std::vector<double> hr(n), hw(n);
+    const double* part = c->b_part.as<double>();
+    CK(cudaMemcpyAsync(hr.data(), part + first * nT * nb, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hw.data(), part + nwork * nT * nb + first * nT * nb, n * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double* R[3] = {rate_pp, rate_pm, rate_mm};
+    double* W[3] = {wp_pp, wp_pm, wp_mm};
+    const double rate_scale = hbarp() * hbarp() * kPi / 8.0 * (double)3.37617087f * 1.e9;
+    for (int ch = 0; ch < 3; ch++)
+        for (int i = 0; i < nb; i++) {
+            double r = 0.0, w = 0.0;
+            for (int q = 0; q < ii1 - ii0; q++) {
+                const size_t o = (((size_t)q * 3 + ch) * nT + t) * nb + i;
+                r += hr[o];
+                w += hw[o];
+            }
+            R[ch][i] = r * rate_scale / S.nptk / S.nptk;
+            W[ch][i] = w / S.nptk / S.nptk;
+        }
+    return FP4_OK;
 }
 
 // Ind_driver_4ph (processes.f90:3551-3822): the ordered index lists of the three

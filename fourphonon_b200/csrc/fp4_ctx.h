@@ -56,6 +56,7 @@ struct fp4_ctx {
     DevBuffer b_harm[6];  // harmonic stage: pair ranges, terms, images, symmetrizers, outputs, born/masses
     IfcTables ifc3, ifc4;
     int64_t last_nproc = 0, last_ncontr = 0, last_launches = 0;
+    int last_rta4_nT = 0;  // temperatures of the last four-phonon RTA call (0: none; its partials are in b_part)
     int64_t last_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double last_ms = 0.0, last_kernel_ms = 0.0;
     std::vector<DevBuffer*> all_buffers() {

@@ -9,6 +9,7 @@
 // statistics and error words, the staged results) lives in one file-scope
 // __device__ array of fixed size, which every GPU that loads the library
 // keeps until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,13 +24,73 @@ using namespace fp4;
 
 namespace {
 
-// 12 MiB: the packed (v, w) table of nptk*nbands modes (32 B each) plus small tables
+// 12 MiB.  A call needs nptk*nbands*32 B (the packed (v, w) table), nptk*4 B (grid
+// coordinates), nlist*4 B (List), nlist*nbands*48 B (staged counts and phase spaces of
+// the three channels) and 256 B of counters, each part rounded up to 256 B.
 constexpr size_t kScratchBytes = 12u << 20;
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
+// The array has one copy per CUDA context, so its device address is looked up once per
+// context, keyed by the context's unique id (cuCtxGetId ids are never reused, unlike
+// CUcontext handles): a host that creates its own context, or resets the device between
+// calls, gets the address that belongs to its current context.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+constexpr int kMaxContexts = 64;
 std::mutex g_setup_mutex;
-unsigned char* g_scratch_addr[kMaxDevices] = {nullptr};
+bool g_entry_points_done = false;
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+unsigned long long g_ctx_ids[kMaxContexts] = {0};
+unsigned char* g_ctx_addr[kMaxContexts] = {nullptr};
+int g_nctx = 0;
+
+// Unique id of the calling thread's current context; false if there is none yet or the
+// driver does not offer the query.  Called with g_setup_mutex held.
+bool current_context_id(unsigned long long* id) {
+    if (!g_entry_points_done) {
+        g_entry_points_done = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(f);
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return g_ctx_get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of g_scratch in the current context (set-up on the first call in each
+// context; the runtime creates the device's context here if it does not exist yet).
+cudaError_t scratch_address(unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    unsigned long long id = 0;
+    const bool have_id = current_context_id(&id);
+    if (have_id)
+        for (int x = 0; x < g_nctx; x++)
+            if (g_ctx_ids[x] == id) {
+                *out = g_ctx_addr[x];
+                return cudaSuccess;
+            }
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
+    if (e != cudaSuccess) return e;
+    if (!ptr) return cudaErrorInvalidSymbol;
+    *out = static_cast<unsigned char*>(ptr);
+    unsigned long long id2 = 0;  // the context may have been created by the lookup itself
+    if (current_context_id(&id2)) {
+        const int slot = (g_nctx < kMaxContexts) ? g_nctx++ : (int)(id2 % kMaxContexts);
+        g_ctx_ids[slot] = id2;
+        g_ctx_addr[slot] = *out;
+    }
+    return cudaSuccess;
+}
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -95,17 +156,9 @@ extern "C" int fp4_np_driver_4ph_noalloc(const fp4_globals* g, const double* ene
     if (need > kScratchBytes) return FP4_E_CAPACITY;
 
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FP4_E_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) return FP4_E_CUDA;
     unsigned char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_addr[dev]) {
-            void* ptr = nullptr;
-            if (cudaGetSymbolAddress(&ptr, g_scratch) != cudaSuccess || !ptr) return FP4_E_CUDA;
-            g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
-        }
-        base = g_scratch_addr[dev];
-    }
+    if (scratch_address(&base) != cudaSuccess) return FP4_E_CUDA;
     int sm_count = 148;
     cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
     cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -88,7 +88,9 @@ class Control:
     eps: float = float(np.float32(1e-5))
     omega_max: float = 1.0e100
     num_sample_process_3ph: int = -1
+    num_sample_process_3ph_phase_space: int = -1
     num_sample_process_4ph: int = -1
+    num_sample_process_4ph_phase_space: int = -1
     flags: dict = field(default_factory=dict)
 
     def crystal(self) -> Crystal:
@@ -182,7 +184,10 @@ def read_control(path_or_text: str, is_text: bool = False) -> Control:
     # namelist names are case-insensitive; map them onto the Control fields
     pmap = {"t": "T", "t_min": "T_min", "t_max": "T_max", "t_step": "T_step", "scalebroad": "scalebroad",
             "maxiter": "maxiter", "eps": "eps", "omega_max": "omega_max",
-            "num_sample_process_3ph": "num_sample_process_3ph", "num_sample_process_4ph": "num_sample_process_4ph"}
+            "num_sample_process_3ph": "num_sample_process_3ph",
+            "num_sample_process_3ph_phase_space": "num_sample_process_3ph_phase_space",
+            "num_sample_process_4ph": "num_sample_process_4ph",
+            "num_sample_process_4ph_phase_space": "num_sample_process_4ph_phase_space"}
     for (k, s, v) in g.get("parameters", []):
         if k in pmap:
             cur = getattr(c, pmap[k])
@@ -202,6 +207,14 @@ def read_control(path_or_text: str, is_text: bool = False) -> Control:
         raise InputError("four_phonon_iteration=.TRUE. but convergence=.FALSE.")
     if flags["four_phonon_iteration"] and not flags["four_phonon"]:
         raise InputError("four_phonon_iteration=.TRUE. but four_phonon=.FALSE.")
+    # the sampling checks of read_config (config.f90:204-221)
+    if not flags["four_phonon"] and (c.num_sample_process_4ph > 0 or c.num_sample_process_4ph_phase_space > 0):
+        raise InputError("four_phonon=.false. but num_sample_process_4ph.gt.0 or "
+                         "num_sample_process_4ph_phase_space.gt.0")
+    if flags["convergence"] and c.num_sample_process_3ph > 0:
+        raise InputError("convergence=.true. but num_sample_process_3ph.gt.0")
+    if flags["four_phonon_iteration"] and c.num_sample_process_4ph > 0:
+        raise InputError("four_phonon_iteration=.true. but num_sample_process_4ph.gt.0")
     c.flags = flags
     return c
 

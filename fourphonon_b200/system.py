@@ -180,7 +180,10 @@ def load_inputs(directory, ctx=None) -> Solve:
         omega, vel, eig = H.eigen_dm(cr, fc, ctl.ngrid, sym.symmetrizers, ctl.born, ctl.epsilon, nac)
     cl3, _ = I.read_fc_anharmonic(path("FORCE_CONSTANTS_3RD"), cr.lattvec, 3)
     ifc4 = None
-    if ctl.flags["four_phonon"] and os.path.exists(path("FORCE_CONSTANTS_4TH")):
+    if ctl.flags["four_phonon"]:
+        # the reference stops when four_phonon is set and read4fc finds no file
+        if not os.path.exists(path("FORCE_CONSTANTS_4TH")):
+            raise I.InputError("four_phonon=.TRUE. but FORCE_CONSTANTS_4TH is missing")
         cl4, _ = I.read_fc_anharmonic(path("FORCE_CONSTANTS_4TH"), cr.lattvec, 4)
         ifc4 = IFC.from_clusters(cl4, cr.lattvec)
     return Solve(cr, tuple(ctl.ngrid), np.asfortranarray(omega), np.asfortranarray(vel), np.asfortranarray(eig), sym,

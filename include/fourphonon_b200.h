@@ -335,12 +335,16 @@ int fp4_eigen_dm(fp4_ctx *ctx, const fp4_globals *g, const double *lattvec, cons
  * array argument is a DEVICE pointer (energy(nptk,nbands),
  * velocity(nptk,nbands,3), List(nlist) in, the six per-mode outputs out);
  * `stream` is a cudaStream_t (NULL: the default stream), synchronised before
- * the call returns.  Scratch lives in one fixed 12 MiB device array that the
- * library holds on every GPU it is loaded on until the process exits; it is
- * enough for nptk*nbands*32 bytes of packed modes plus small tables (e.g. a
- * 24^3 grid with 12 branches).  Larger systems return FP4_E_CAPACITY.  The
- * first call on a device looks up the array's device address, so make that
- * call before any stream capture.  All calls share the array: calls that
+ * the call returns.  Scratch lives in one fixed 12 MiB (12,582,912 B) device
+ * array that the library holds on every GPU it is loaded on until the process
+ * exits.  A call needs nptk*nbands*32 + nptk*4 + nlist*4 + nlist*nbands*48
+ * bytes plus 256 B of counters, each of the five parts rounded up to 256 B:
+ * e.g. a 24^3 grid with 12 branches fits when List is an irreducible wedge
+ * (nlist up to about 8,000 points) but not the full grid.  Larger calls
+ * return FP4_E_CAPACITY before any device work; a List entry outside
+ * [1, nptk] returns FP4_E_ARG.  The first call in each CUDA context looks up
+ * the array's device address in that context, so make that call before any
+ * stream capture.  All calls share the array: calls that
  * overlap on the GPU (other threads, other streams) race and must be
  * serialised by the caller.  No cudaMalloc/cudaFree is ever called.
  */
@@ -348,6 +352,18 @@ int fp4_np_driver_4ph_noalloc(const fp4_globals *g, const double *energy, const 
                               const int32_t *list, int64_t *n_plusplus, double *pspace_plusplus, int64_t *n_plusminus,
                               double *pspace_plusminus, int64_t *n_minusminus, double *pspace_minusminus,
                               void *stream);
+
+/*
+ * Inspection of the last four-phonon RTA call (fp4_rta_driver_4ph[_multi_t]):
+ * for irreducible point ll (0-based) and temperature index t, the rates and
+ * WP4 of each branch (nbands values per output) from the processes whose
+ * second phonon q' lies in [ii0, ii1) (0-based grid indices), normalised as
+ * the full driver normalises them.  Over a partition of the grid these sum to
+ * the driver's outputs.  No counterpart in the reference: it lets a large
+ * grid be checked against a CPU restatement of a few q' points.
+ */
+int fp4_rta4_partials(fp4_ctx *ctx, int32_t ll, int32_t ii0, int32_t ii1, int32_t t, double *rate_pp,
+                      double *rate_pm, double *rate_mm, double *wp_pp, double *wp_pm, double *wp_mm);
 
 /*
  * Work counters of the last four-phonon call: [0] surviving processes,

@@ -677,6 +677,33 @@ void fp4o_ind4(const fp4o_sys *s, const fp4o_ifc *f, const int64_t *n_pp, const 
 }
 
 /*
+ * RTA_driver_4ph restricted to the q' points [ii0,ii1) (0-based): for modes
+ * [mm0,mm1) the per-channel rates and WP4 of the processes whose second phonon
+ * lies in the range, normalised as the full driver normalises them
+ * (processes.f90:3828-4129, 5256).  Summed over a partition of the grid into
+ * ranges this is the full RTA_driver_4ph (up to summation order); it checks a
+ * large grid where the full sums take too long on the CPU.
+ */
+void fp4o_rta4_range(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int ii0, int ii1, double *rate_pp,
+                     double *rate_pm, double *rate_mm, double *wp_pp, double *wp_pm, double *wp_mm) {
+    double *R[3] = {rate_pp, rate_pm, rate_mm}, *W[3] = {wp_pp, wp_pm, wp_mm};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int x = 0; x < 3 * (mm1 - mm0); x++) {
+        int ch = x % 3, m0 = mm0 + x / 3;
+        R[ch][m0] = 0.0;
+        W[ch][m0] = 0.0;
+        if (!gate(s, m0 + 1)) continue;
+        acc4_t a;
+        memset(&a, 0, sizeof a);
+        a.ii0 = ii0;
+        a.ii1 = ii1;
+        proc4_one(s, f, m0 + 1, ch, 2, &a);
+        R[ch][m0] = a.gamma;
+        W[ch][m0] = a.wp;
+    }
+}
+
+/*
  * Bounded sample of RTA_driver_4ph for timing: modes [mm0,mm1), each
  * restricted to the q' range [ii0,ii1).  Returns the number of surviving
  * processes visited; rates are not normalised (timing use only).

@@ -144,6 +144,14 @@ class Oracle:
         lib().fp4o_rta4(ct.byref(self.sys), ct.byref(self.ifc4), mm0, mm1, *[_p(x) for x in out])
         return out  # rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm
 
+    def rta4_range(self, mm0, mm1, ii0, ii1):
+        """RTA_driver_4ph over modes [mm0,mm1) restricted to q' in [ii0,ii1) (0-based),
+        normalised as the full driver: rate_pp, rate_pm, rate_mm, wp_pp, wp_pm, wp_mm."""
+        nm = self.s.nmodes
+        out = [np.zeros(nm) for _ in range(6)]
+        lib().fp4o_rta4_range(ct.byref(self.sys), ct.byref(self.ifc4), mm0, mm1, ii0, ii1, *[_p(x) for x in out])
+        return out
+
     def rta4_sample(self, mm0, mm1, ii0, ii1):
         """Timing sample: RTA_driver_4ph work for modes [mm0,mm1) restricted to
         q' in [ii0,ii1); returns the number of surviving processes visited."""
