@@ -39,6 +39,20 @@ METRIC = "4ph processes/s"
 UNIT = "processes/s"
 WORKLOAD = "diamond 2-atom fcc a=5.43A, 16x16x16 q-grid, 3ph+4ph, 4ph RTA at T={300,700}K fused, scalebroad=1"
 
+# The workloads: 1 is the benchmarked one (the default); 0, 2 and 3 are the
+# other cells of the task, timed the same way when asked for with --config.
+CONFIGS = {
+    0: dict(kind="diamond", grid=6, temps=(300.0,),
+            workload="diamond 2-atom fcc a=5.43A, 6x6x6 q-grid, 4ph RTA at T=300K, scalebroad=1"),
+    1: dict(kind="diamond", grid=16, temps=(300.0, 700.0), workload=WORKLOAD),
+    2: dict(kind="layered", grid=12, temps=(300.0,),
+            workload="R-3m 4-atom layered cell (masses 6.94/58.93/16/16, a=2.82A, c/a=5), 12 branches, 12x12x12, "
+                     "4th-order cutoff at the 2nd shell, 4ph RTA at T=300K"),
+    3: dict(kind="zincblende", grid=24, temps=(100.0, 300.0, 500.0, 1000.0),
+            workload="zincblende 2-atom a=4.78A masses 10.81/74.92, 24x24x24, 4ph RTA at T={100,300,500,1000}K "
+                     "in one launch; full enumeration, and 2e6 sampled processes per mode and channel"),
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -46,11 +60,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--grid", type=int, default=16, help="q-grid edge (16 = the benchmarked workload)")
+    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS),
+                    help="workload (1 = the benchmarked 16^3 diamond solve)")
+    ap.add_argument("--grid", type=int, default=None, help="override the q-grid edge of the workload")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-sampled", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=64)
     return ap.parse_args()
 
@@ -62,16 +79,24 @@ def log(*a):
 # ---------------------------------------------------------------------------- workload
 
 
-def workload(grid, rank=0):
+def config_of(args):
+    c = dict(CONFIGS[args.config])
+    if args.grid:
+        c["grid"] = args.grid
+        c["workload"] = c["workload"] + f" (grid overridden: {args.grid}^3)"
+    return c
+
+
+def workload(cfg, rank=0):
     from fourphonon_b200 import system as S
 
-    temps = (300.0 + 10.0 * rank, 700.0 + 10.0 * rank)
-    base = S.cached_solve("diamond", (grid, grid, grid), temperatures=(300.0, 700.0))
+    g = cfg["grid"]
+    base = S.cached_solve(cfg["kind"], (g, g, g), temperatures=tuple(cfg["temps"]))
     if rank:
         import copy
 
         s = copy.copy(base)
-        s.temperatures = list(temps)
+        s.temperatures = [t + 10.0 * rank for t in cfg["temps"]]
         return s
     return base
 
@@ -206,10 +231,14 @@ def all_sum(world, x):
 # ---------------------------------------------------------------------------- CPU baseline (oracle)
 
 
-def cpu_sample(s, target_s=15.0):
-    """Time the oracle (the C restatement of RTA_driver_4ph, OpenMP over modes)
-    on a bounded sample: modes of the second irreducible q-point onward, each
-    restricted to the q' points 2..1+n; the sample is sized to ~target_s."""
+def cpu_sample(s, target_s=15.0, full=False):
+    """Time the oracle (the C restatement of RTA_driver_4ph, OpenMP over modes
+    and q' points) on the workload.  full=True times the whole driver (every
+    mode, all three channels, first temperature).  Otherwise a bounded sample
+    spread over the whole workload: every mode of the irreducible wedge (Gamma
+    included), each over every stride-th q' point, the stride chosen so the
+    sample takes about target_s; processes/s of the sample stand for the whole
+    (per-process cost does not depend on q', and every mode is in it)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -217,19 +246,31 @@ def cpu_sample(s, target_s=15.0):
     threads = lib.fp4o_num_threads()
     o = O.Oracle(s, T=s.temperatures[0])
     nm = s.nmodes
-    mm0 = s.nb  # skip the Gamma point
-    nmodes = min(nm - mm0, max(threads, 1) * 2)
+    if full:
+        t0 = time.perf_counter()
+        o.rta4()
+        dt = time.perf_counter() - t0
+        n = int(sum(x.sum() for x in O.Oracle(s).np4()[0]))
+        return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": f"full oracle RTA_driver_4ph restatement: all {nm} modes, all q' points, three channels, "
+                          f"T={s.temperatures[0]:.0f} K: {n} processes in {dt:.1f} s", "processes": n, "seconds": dt}
+    modes = np.arange(nm)
+    # a probe at a coarse stride sizes the sample
+    stride = max(1, s.nptk // 2)
     t0 = time.perf_counter()
-    n = o.rta4_sample(mm0, mm0 + nmodes, 1, 2)
-    dt = time.perf_counter() - t0
-    per_ii = max(dt, 1e-3)
-    nii = int(max(1, min(s.nptk, target_s / per_ii)))
+    o.rta4_strided(modes, stride, 1)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    per_q = dt / max(1, len(range(1, s.nptk, stride)))
+    nq = int(max(1, min(s.nptk, target_s / per_q)))
+    stride = max(1, s.nptk // nq)
     t0 = time.perf_counter()
-    n = o.rta4_sample(mm0, mm0 + nmodes, 1, 1 + nii)
+    n = o.rta4_strided(modes, stride, 1)
     dt = time.perf_counter() - t0
+    nqs = len(range(1, s.nptk, stride))
     return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"oracle RTA_driver_4ph restatement, {nmodes} modes x q' points 2..{1 + nii} "
-                      f"(all three channels, T={s.temperatures[0]:.0f} K): {n} processes in {dt:.1f} s",
+            "sample": f"oracle RTA_driver_4ph restatement, all {nm} modes x {nqs} q' points (every {stride}th from "
+                      f"the 2nd), three channels, T={s.temperatures[0]:.0f} K: {n} processes in {dt:.1f} s "
+                      f"({100.0 * nqs / s.nptk:.1f}% of the q' points; processes/s of the sample stand for the whole)",
             "processes": n, "seconds": dt}
 
 
@@ -237,13 +278,15 @@ def run_reference(args):
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
         return 0
-    s = workload(args.grid)
+    cfg = config_of(args)
+    s = workload(cfg)
+    full = args.config == 0
     vals = []
     for w in range(args.warmup):
-        cpu_sample(s, target_s=2.0)
+        cpu_sample(s, target_s=2.0, full=False)
     samples = []
     for k in range(args.steps):
-        r = cpu_sample(s, target_s=10.0)
+        r = cpu_sample(s, target_s=10.0, full=full)
         samples.append(r)
         vals.append(r["value"])
     v = float(np.mean(vals))
@@ -251,7 +294,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample": samples[-1]["sample"]},
+            "config": {"workload": cfg["workload"], "sample": samples[-1]["sample"]},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": samples[-1]["cores"], "kind": "port",
                              "sample": samples[-1]["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -341,20 +384,80 @@ def rta_kappa(ctx, s, rate_total, t):
     return float(np.trace(k) / 3.0)
 
 
+def bf16_peak():
+    """Measured dense bf16 peak (burst) in TFLOP/s and where it came from."""
+    fn = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(fn):
+        try:
+            d = json.load(open(fn))
+            for k in ("bf16_tflops", "bf16_dense_tflops"):
+                if k in d:
+                    return float(d[k]), "measured (MEASURED_PEAKS.json bf16 burst)"
+        except (ValueError, OSError):
+            pass
+    return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json on this box)"
+
+
+def run_mixed(torch, world, dev, stream, s, args, flush, precision, ref_last, ref_value, ctx64):
+    """The same workload in one of the mixed precisions: throughput, its speed-up
+    over FP64, the per-mode rate and kappa errors against the FP64 driver."""
+    from fourphonon_b200 import abi
+
+    cmx = abi.Context(dev, precision)
+    cmx.set_stream(stream.cuda_stream)
+    for _ in range(max(1, args.warmup)):
+        cmx.rta_driver_4ph(s)
+    torch.cuda.synchronize()
+    barrier(world)
+    rmx = time_steps(torch, cmx, s, args.steps, flush)
+    barrier(world)
+    tmx = all_max(world, sum(r["ms"] for r in rmx) / 1e3)
+    vmx = all_sum(world, sum(r["nproc"] for r in rmx)) / tmx
+    cnt = rmx[-1]["counters"]
+    cmx.close()
+    r3 = ctx64.rta_driver(s)["rate"]
+    kerr, rate_err = [], []
+    for t in range(len(s.temperatures)):
+        r64 = ref_last["rates"]["rate_4ph"][t]
+        rm = rmx[-1]["rates"]["rate_4ph"][t]
+        k64 = rta_kappa(ctx64, s, r3 + r64, t)
+        kmx = rta_kappa(ctx64, s, r3 + rm, t)
+        k64_4 = rta_kappa(ctx64, s, r64, t)
+        kmx_4 = rta_kappa(ctx64, s, rm, t)
+        kerr.append(max(abs(kmx - k64) / abs(k64), abs(kmx_4 - k64_4) / abs(k64_4)))
+        m = r64 > 1e-6 * r64.max()
+        rate_err.append(float(np.max(np.abs(rm[m] - r64[m]) / r64[m])))
+    kms = float(np.mean([r["kms"] for r in rmx]))
+    out = {"value": vmx, "unit": UNIT, "speedup_vs_fp64": vmx / ref_value, "kappa_rel_err": max(kerr),
+           "rate_rel_err_max": max(rate_err), "kernel_ms": kms, "tensor_cores": bool(cnt[7])}
+    if cnt[7]:
+        tflops = cnt[6] * 65536.0 / (kms / 1e3) / 1e12
+        peak, note = bf16_peak()
+        out["dtype"] = "split-bf16 (hi*hi+hi*lo+lo*hi) tcgen05 products, FP32 accumulation in TMEM; FP64 filter/weights/sums"
+        out["roofline"] = {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                           "frac": tflops / peak, "kernel": "k4_work_tc", "peak_note": note,
+                           "achieved_note": "tensor-core flops issued (work counter 6 x 65536) / event-timed kernel "
+                                            "duration; the kernel is bound by its FP64 filter, not by the products"}
+    else:
+        out["dtype"] = "FP32 contraction on the CUDA cores; FP64 filter/weights/sums"
+    return out
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     import torch
 
     from fourphonon_b200 import abi
 
+    cfg = config_of(args)
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
     # rank 0 builds (and caches) the synthetic solve first
     if rank == 0:
-        s = workload(args.grid, rank)
+        s = workload(cfg, rank)
     barrier(world)
     if rank != 0:
-        s = workload(args.grid, rank)
+        s = workload(cfg, rank)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     ctx = abi.Context(dev, abi.FP4_PREC_FP64)
@@ -386,35 +489,10 @@ def run_ours(args):
     launches = sum(r["launches"] for r in res)
 
     out = {}
-    # mixed precision (same workload, FP32 contraction)
     if not args.no_mixed:
-        cmx = abi.Context(dev, abi.FP4_PREC_MIXED)
-        cmx.set_stream(stream.cuda_stream)
-        for _ in range(max(1, args.warmup)):
-            cmx.rta_driver_4ph(s)
-        torch.cuda.synchronize()
-        barrier(world)
-        rmx = time_steps(torch, cmx, s, args.steps, flush)
-        barrier(world)
-        tmx = all_max(world, sum(r["ms"] for r in rmx) / 1e3)
-        vmx = all_sum(world, sum(r["nproc"] for r in rmx)) / tmx
-        r3 = ctx.rta_driver(s)["rate"]
-        kerr = []
-        rate_err = []
-        for t in range(len(s.temperatures)):
-            r64 = last["rates"]["rate_4ph"][t]
-            rm = rmx[-1]["rates"]["rate_4ph"][t]
-            k64 = rta_kappa(ctx, s, r3 + r64, t)
-            kmx = rta_kappa(ctx, s, r3 + rm, t)
-            k64_4 = rta_kappa(ctx, s, r64, t)
-            kmx_4 = rta_kappa(ctx, s, rm, t)
-            kerr.append(max(abs(kmx - k64) / abs(k64), abs(kmx_4 - k64_4) / abs(k64_4)))
-            m = r64 > 1e-6 * r64.max()
-            rate_err.append(float(np.max(np.abs(rm[m] - r64[m]) / r64[m])))
-        out["mixed"] = {"value": vmx, "unit": UNIT, "speedup_vs_fp64": vmx / value, "kappa_rel_err": max(kerr),
-                        "rate_rel_err_max": max(rate_err), "dtype": "f32 contraction, f64 filter/weights/reductions",
-                        "kernel_ms": float(np.mean([r["kms"] for r in rmx]))}
-        cmx.close()
+        out["mixed"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED, last, value, ctx)
+        out["mixed_simt"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED_SIMT, last, value,
+                                      ctx)
 
     # end to end through the public API with host buffers (no upload cache)
     if not args.no_e2e:
@@ -438,19 +516,21 @@ def run_ours(args):
                       "d2h_bytes_per_step": int(d2h)}
         ce.close()
 
-    if rank == 0 and world == 1 and not args.no_serve:
+    if args.config == 3 and not args.no_sampled:
+        out["sampled"] = run_sampled(torch, ctx, s, last, flush, 1000.0 * t_max / args.steps)
+    if rank == 0 and world == 1 and not args.no_serve and args.config == 1:
         out["serving"] = run_serving(args)
     peak = fp64_dgemm_peak(torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(s, target_s=15.0)
+        cpu = cpu_sample(s, target_s=15.0, full=(args.config == 0))
     ctx.close()
     if rank != 0:
         barrier(world)
         return 0
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k4_work_diamond16.txt")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and args.config == 1:
         for line in open(tf):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
@@ -458,7 +538,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "temperatures_K": s.temperatures, "nmodes": s.nmodes,
+        "config": {"workload": cfg["workload"], "config_index": args.config, "grid": [cfg["grid"]] * 3,
+                   "temperatures_K": s.temperatures, "nmodes": s.nmodes, "nbands": s.nb,
                    "ntri4": s.ifc4.ntri, "displacement_classes": npi, "processes_per_step": last["nproc"],
                    "contracted_per_step": last["ncontr"],
                    "work_counters": {"sigma_evals": int(cnt[2]), "window_tests": int(cnt[3]),
@@ -468,7 +549,7 @@ def run_ours(args):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
                      "kernel": "k4_work", "kernel_ms": kms,
-                     "peak_note": "FP64: cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe peak; no FP64 figure in "
+                     "peak_note": "FP64: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
                                   "MEASURED_PEAKS)",
                      "achieved_note": "executed FP64 flops of k4_work from its work counters / event-timed duration",
                      "ref_equivalent_tflops": last["nproc"] * ref_flops_per_process(s) / (kms / 1e3) / 1e12},
@@ -483,6 +564,29 @@ def run_ours(args):
 
         dist.destroy_process_group()
     return 0
+
+
+def run_sampled(torch, ctx, s, full, flush, full_ms, nsamples=2_000_000, seed=20240605):
+    """The sampled estimator of the same workload (FP64): its time and the error
+    of its rates against the full enumeration, summed over modes and per mode."""
+    flush.zero_()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r = ctx.rta_driver_4ph_sample(s, nsamples, seed)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    errs = {}
+    for t, T in enumerate(s.temperatures):
+        f = full["rates"]["rate_4ph"][t]
+        g = r["rate_plusplus"][t] + r["rate_plusminus"][t] + r["rate_minusminus"][t]
+        m = f > 1e-6 * f.max()
+        rel = np.abs(g[m] - f[m]) / f[m]
+        errs[f"{T:.0f}K"] = {"sum_rel_err": float(abs(g.sum() - f.sum()) / f.sum()),
+                             "per_mode_median": float(np.median(rel)), "per_mode_p90": float(np.percentile(rel, 90))}
+    return {"nsamples_per_mode_channel": nsamples, "ms": ms, "speedup_vs_full": full_ms / ms,
+            "errors_vs_full": errs, "dtype": "f64"}
 
 
 # ---------------------------------------------------------------------------- serving stream

@@ -34,6 +34,7 @@ _lib = None
 
 FP4_PREC_FP64 = 0
 FP4_PREC_MIXED = 1
+FP4_PREC_MIXED_SIMT = 2
 FP4_OK = 0
 FP4_E_ARG = -1
 FP4_E_CUDA = -2
@@ -76,6 +77,20 @@ def load(build_if_missing: bool = True):
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+def tc_selftest(A_bf16: np.ndarray, B_bf16: np.ndarray) -> np.ndarray:
+    """D = A B^T on the tensor cores (fp4_tc_selftest): A (128, K) and B (N, K)
+    as raw bf16 bits (uint16), D (128, N) float32."""
+    lib = load()
+    A = np.ascontiguousarray(A_bf16, dtype=np.uint16)
+    B = np.ascontiguousarray(B_bf16, dtype=np.uint16)
+    assert A.shape[0] == 128 and A.shape[1] == B.shape[1]
+    D = np.zeros((128, B.shape[0]), dtype=np.float32)
+    rc = lib.fp4_tc_selftest(ct.c_int32(A.shape[1]), ct.c_int32(B.shape[0]), _p(A), _p(B), _p(D))
+    if rc != 0:
+        raise FP4Error(rc, "fp4_tc_selftest failed")
+    return D
 
 
 class Context:

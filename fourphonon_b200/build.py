@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfp4b200.so")
-SOURCES = ["fp4_abi.cu", "fp4_rates.cu", "fp4_rates4.cu", "fp4_bte.cu", "fp4_noalloc.cu", "fp4_serve.cu", "fp4_sample.cu", "fp4_harmonic.cu"]
+SOURCES = ["fp4_abi.cu", "fp4_rates.cu", "fp4_rates4.cu", "fp4_bte.cu", "fp4_noalloc.cu", "fp4_serve.cu", "fp4_sample.cu", "fp4_harmonic.cu",
+           "fp4_tc_check.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++"]

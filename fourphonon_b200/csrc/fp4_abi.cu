@@ -129,7 +129,7 @@ extern "C" const char* fp4_last_error(const fp4_ctx* c) { return c ? c->err.c_st
 
 extern "C" int fp4_set_precision(fp4_ctx* c, int precision) {
     if (!c) return FP4_E_ARG;
-    if (precision != FP4_PREC_FP64 && precision != FP4_PREC_MIXED)
+    if (precision != FP4_PREC_FP64 && precision != FP4_PREC_MIXED && precision != FP4_PREC_MIXED_SIMT)
         return fp4_fail(c, FP4_E_ARG, "unknown precision %d", precision);
     c->precision = precision;
     return FP4_OK;
@@ -374,6 +374,7 @@ int fp4_setup_ifc(fp4_ctx* c, const fp4_globals* g, int order, int32_t ntri, con
     if ((r = T.cl_index.upload(c, cl_index.data(), ntri * sizeof(int)))) return r;
     if ((r = T.pi_d.upload(c, pi_d.data(), npi * sizeof(int4)))) return r;
     if ((r = T.blk_start.upload(c, blk_start.data(), (nat * nat + 1) * sizeof(int)))) return r;
+    T.h_blk_start = blk_start;
     DevIfc& F = T.F;
     F.order = order;
     F.ntri = ntri;
@@ -403,6 +404,7 @@ int fp4_begin(fp4_ctx* c) {
     if ((r = c->b_stats.reserve(c, 64))) return r;
     c->launches = 0;
     c->kernel_timed = false;
+    c->last_tc = false;
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaMemsetAsync(c->b_err.ptr, 0, 64, c->stream));
     CK(cudaMemsetAsync(c->b_stats.ptr, 0, 64, c->stream));
@@ -429,9 +431,11 @@ int fp4_end(fp4_ctx* c) {
     c->last_nproc = (int64_t)st[0];
     c->last_ncontr = (int64_t)st[1];
     for (int x = 0; x < 8; x++) c->last_counters[x] = (int64_t)st[x];
+    c->last_counters[7] = c->last_tc ? 1 : 0;
     if (flags & kErrQueue) return fp4_fail(c, FP4_E_CAPACITY, "an output list or work queue was smaller than the process count");
     if (flags & kErrTable) return fp4_fail(c, FP4_E_CAPACITY, "a device table limit was exceeded");
     if (flags & kErrList) return fp4_fail(c, FP4_E_ARG, "a process list entry is out of range or breaks momentum conservation");
+    if (flags & kErrTimeout) return fp4_fail(c, FP4_E_TIMEOUT, "a bounded wait for the tensor core gave up");
     return FP4_OK;
 }
 
@@ -666,7 +670,7 @@ extern "C" int fp4_ind_driver(fp4_ctx* c, const fp4_globals* g, const double* en
 // four-phonon drivers
 // ---------------------------------------------------------------------------
 static int k4_blocks(fp4_ctx* c, int nwork, int kind, int nT) {
-    int nbk = c->sm_count * k4_ctas_per_sm(kind, nT, c->precision == FP4_PREC_MIXED);
+    int nbk = c->sm_count * k4_ctas_per_sm(kind, nT, c->precision != FP4_PREC_FP64);
     return std::max(1, std::min(nbk, nwork));
 }
 
@@ -785,26 +789,67 @@ static int k4_queue(fp4_ctx* c, int nblocks, bool with_pos, P4Params& p) {
 }
 
 // Four-phonon RTA at nT temperatures; outputs device-resident in c->b_out4 as (nb,nlist,nT) x 6.
+// The tensor-core plan of the four-phonon RTA call, if the mixed precision asks for
+// it and its tables fit in shared memory: zbins as large as keeps two CTAs per SM
+// (else one); returns false when the CUDA-core FP32 contraction has to run instead.
+static bool k4_tc_setup(fp4_ctx* c, int nT, int subcap, TcPlan& plan, size_t& smem, int& ctas) {
+    const DevSys& S = c->S;
+    const DevIfc& F = c->ifc4.F;
+    if (c->precision != FP4_PREC_MIXED || S.onlyharmonic) return false;
+    if (k4_tc_plan(S.nb, S.natoms, F.npi, c->ifc4.h_blk_start.data(), subcap, plan) != 0) return false;
+    const size_t per_sm = 228 * 1024, per_cta_max = 227 * 1024;
+    const int base_cap = plan.chunk_cap;
+    for (int zb = 8; zb >= 1; zb--) {
+        TcPlan q = plan;
+        q.zbins = zb;
+        q.chunk_cap = zb * base_cap;
+        const size_t need = k4_tc_smem(nT, S, F, q);
+        if (2 * (need + 1024) <= per_sm || (zb == 1 && need <= per_cta_max)) {
+            plan = q;
+            smem = need;
+            ctas = (2 * (need + 1024) <= per_sm) ? 2 : 1;
+            return true;
+        }
+    }
+    return false;
+}
+
 int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     if (nT < 1 || nT > kMaxTemps) return fp4_fail(c, FP4_E_ARG, "nT=%d outside [1,%d]", nT, kMaxTemps);
     for (int t = 0; t < nT; t++)
         if (!(temps[t] > 0.0)) return fp4_fail(c, FP4_E_ARG, "T must be >0 K");
     const DevSys& S = c->S;
     const int nm = S.nb * S.nlist;
-    const bool mixed = (c->precision == FP4_PREC_MIXED);
+    const bool mixed = (c->precision != FP4_PREC_FP64);
     size_t sm = k4_smem(2, nT, mixed, S, c->ifc4.F);
-    if (sm > 227 * 1024)
-        return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);
+    const int nwork = 3 * S.nlist * S.nptk;
+    // the queue is sized for the larger of the two grids; the tensor-core plan needs its capacity
+    int nblocks = k4_blocks(c, nwork, 2, nT);
+    P4Params p{};
     int r;
+    if ((r = k4_queue(c, std::max(nblocks, c->sm_count * k4_tc_ctas_per_sm()), false, p))) return r;
+    TcPlan plan{};
+    size_t tc_smem = 0;
+    int tc_ctas = 0;
+    const bool use_tc = k4_tc_setup(c, nT, p.subcap, plan, tc_smem, tc_ctas);
+    if (!use_tc && sm > 227 * 1024)
+        return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);
+    if (use_tc) nblocks = std::max(1, std::min(nwork, c->sm_count * tc_ctas));
+    c->last_tc = use_tc;
     if ((r = c->b_temps.upload(c, temps, nT * sizeof(double)))) return r;
     const int wbs = wb_stride(k4_round_nt(nT));
     if ((r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wbs * sizeof(double)))) return r;
     CK(launch_wbose(S, c->b_temps.as<double>(), nT, wbs, c->b_wb.as<double>(), c->stream));
     c->launches++;
-    const int nwork = 3 * S.nlist * S.nptk;
-    const int nblocks = k4_blocks(c, nwork, 2, nT);
-    P4Params p{};
-    if ((r = k4_queue(c, nblocks, false, p))) return r;
+    if (use_tc) {
+        if ((r = c->b_tcplan.reserve(c, sizeof(TcPlan)))) return r;
+        CK(cudaMemcpyAsync(c->b_tcplan.ptr, &plan, sizeof(TcPlan), cudaMemcpyHostToDevice, c->stream));
+        if ((r = c->b_wtab.reserve(c, (size_t)2 * S.nptk * plan.ksteps * 16 * sizeof(uint16_t)))) return r;
+        CK(launch_k4_wtab(S, c->ifc4.F, c->b_tcplan.as<TcPlan>(), plan.ksteps, c->b_wtab.as<uint16_t>(), c->stream));
+        c->launches++;
+        p.tc = c->b_tcplan.as<TcPlan>();
+        p.wtab = c->b_wtab.as<uint16_t>();
+    }
     if ((r = c->b_part.reserve(c, (size_t)nwork * nT * S.nb * 2 * sizeof(double)))) return r;
     if ((r = c->b_work.reserve(c, 64))) return r;
     if ((r = c->b_out4.reserve(c, (size_t)nm * nT * 6 * sizeof(double)))) return r;
@@ -820,7 +865,10 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     p.stats = c->b_stats.as<unsigned long long>();
     p.err = c->b_err.as<int>();
     CK(cudaEventRecord(c->evk0, c->stream));
-    CK(launch_k4(2, nT, mixed, p, nblocks, c->stream));
+    if (use_tc)
+        CK(launch_k4_tc(nT, p, tc_smem, nblocks, c->stream));
+    else
+        CK(launch_k4(2, nT, mixed, p, nblocks, c->stream));
     CK(cudaEventRecord(c->evk1, c->stream));
     c->kernel_timed = true;
     c->launches++;
@@ -917,7 +965,7 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
     if ((r = fp4_setup_ifc(c, g, 4, ntri, psi, r_j, r_k, r_l, index_i, index_j, index_k, index_l, c->ifc4))) return r;
     const DevSys& S = c->S;
     const int nm = S.nb * nlist;
-    const bool mixed = (c->precision == FP4_PREC_MIXED);
+    const bool mixed = (c->precision != FP4_PREC_FP64);
     size_t sm = k4_smem(3, 1, mixed, S, c->ifc4.F);
     if (sm > 227 * 1024)
         return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);

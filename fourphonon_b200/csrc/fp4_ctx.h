@@ -30,6 +30,7 @@ struct DevBuffer {
 struct IfcTables {
     DevBuffer phi, atoms, mj, mk, ml, mu, cl_start, cl_index, pi_d, blk_start;
     fp4::DevIfc F{};
+    std::vector<int> h_blk_start;  // host copy of the classes' block ranges
     std::vector<DevBuffer*> list() { return {&phi, &atoms, &mj, &mk, &ml, &mu, &cl_start, &cl_index, &pi_d, &blk_start}; }
 };
 
@@ -52,6 +53,8 @@ struct fp4_ctx {
     DevBuffer b_energy, b_velocity, b_wv, b_eigraw, b_eig, b_eigf, b_list, b_qc, b_root[3], b_rootf[3];
     DevBuffer b_temps, b_bose, b_wb, b_out, b_out4, b_lists, b_gamma, b_off, b_counts;
     DevBuffer b_queue, b_part, b_work, b_err, b_stats;
+    DevBuffer b_tcplan, b_wtab;  // tensor-core contraction: its plan and phase rows
+    bool last_tc = false;        // the last four-phonon RTA call ran its contraction on the tensor cores
     DevBuffer b_bte[12];
     DevBuffer b_harm[6];  // harmonic stage: pair ranges, terms, images, symmetrizers, outputs, born/masses
     IfcTables ifc3, ifc4;
@@ -62,7 +65,8 @@ struct fp4_ctx {
     std::vector<DevBuffer*> all_buffers() {
         std::vector<DevBuffer*> v = {&b_qc, &b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,
                                      &b_temps,  &b_bose,     &b_wb, &b_out, &b_out4,   &b_lists, &b_gamma, &b_off,
-                                     &b_counts, &b_queue,    &b_part, &b_work,  &b_err,   &b_stats};
+                                     &b_counts, &b_queue,    &b_part, &b_work,  &b_err,   &b_stats,
+                                     &b_tcplan, &b_wtab};
         for (int d = 0; d < 3; d++) {
             v.push_back(&b_root[d]);
             v.push_back(&b_rootf[d]);

@@ -270,6 +270,7 @@ __device__ __forceinline__ void unpack_proc(unsigned long long e, int& a, int& b
 }
 
 // Error flags raised by kernels (read back by the host after each call)
-enum : int { kErrQueue = 1, kErrTable = 2, kErrList = 4 };
+// kErrTimeout: a bounded wait for the tensor core gave up (the kernel stopped early).
+enum : int { kErrQueue = 1, kErrTable = 2, kErrList = 4, kErrTimeout = 8 };
 
 }  // namespace fp4

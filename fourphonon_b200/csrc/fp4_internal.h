@@ -29,6 +29,33 @@ struct P3Params {
     int* err;
 };
 
+// Plan of the tensor-core contraction (mixed precision, RTA): how the
+// displacement classes are laid out along K and the atom-pair blocks along N.
+// Classes run in block order; consecutive non-empty blocks are grouped into
+// passes of at most kTcPassBlocks blocks (32 accumulator columns each: 9 real
+// parts, 9 imaginary parts, padding).  A pass's K range holds 6 values per
+// class, (w_hi.re, w_hi.im, w_hi.re, w_hi.im, w_lo.re, w_lo.im), padded to a
+// multiple of 16, so that one product over K gives
+//   sum_p (w_hi Z_hi + w_hi Z_lo + w_lo Z_hi) ~ sum_p w_p Z_p.
+constexpr int kTcPassBlocks = 4;
+constexpr int kTcMaxBlocks = (kMaxNb / 3) * (kMaxNb / 3);
+constexpr int kTcMaxPass = kTcMaxBlocks;
+constexpr int kTcRows = 128;      // processes per product (the M of one tcgen05.mma)
+constexpr int kTcRegionCols = 128;  // accumulator columns of one warpgroup's TMEM region
+struct TcPlan {
+    int npass;      // passes
+    int ksteps;     // K-steps (16 values each) of one A row over all passes
+    int bin_bytes;  // bytes of one (i,j) bin's B table (all passes)
+    int zbins;      // bins whose tables are built together
+    int nblk;       // non-empty atom-pair blocks
+    int chunk_cap;  // capacity of the chunk list of one group of bins
+    int pass_blk0[kTcMaxPass + 1];    // non-empty blocks [pass_blk0[x], pass_blk0[x+1]) form pass x
+    int pass_cls0[kTcMaxPass + 1];    // first class of each pass
+    int pass_kstep0[kTcMaxPass + 1];  // first K-step of each pass inside an A row
+    int pass_boff[kTcMaxPass + 1];    // byte offset of each pass inside a bin's B table
+    int4 blk[kTcMaxBlocks];           // (first class, end class, atom of the 3rd phonon, atom of the 4th)
+};
+
 struct P4Params {
     DevSys S;
     DevIfc F;
@@ -56,6 +83,10 @@ struct P4Params {
     double* gamma_out[3];
     double gamma_scale;     // hbarp^2 pi/8 * 3.37617087 * 1e9 / nptk^2
     long long* queue_pos;   // list position of each queued process, same indexing as queue
+    // tensor-core contraction: its plan and the A rows (bf16 hi/lo phases) of every q''
+    // for the two channel signs, [sign][q''][ksteps*16]
+    const TcPlan* tc;
+    const uint16_t* wtab;
 };
 
 // One launch of the multi-solve kernel: ranges of work items, each of one solve slot.
@@ -100,6 +131,13 @@ __host__ __device__ constexpr int wb_stride(int NT) { return (NT + 2) & ~1; }
 int k4_round_nt(int nT);  // the temperature count the four-phonon kernels are instantiated for (1, 2, 4, 8)
 cudaError_t launch_wbose(const DevSys& S, const double* T, int nT, int stride, double* wb, cudaStream_t st);
 cudaError_t prepare_k4_multi(bool mixed, size_t smem);
+// tensor-core contraction (mixed precision, RTA)
+int k4_tc_plan(int nb, int natoms, int npi, const int* blk_start_host, int subcap, TcPlan& plan);
+size_t k4_tc_smem(int nT, const DevSys& S, const DevIfc& F, const TcPlan& plan);
+int k4_tc_ctas_per_sm();
+cudaError_t launch_k4_tc(int nT, const P4Params& p, size_t smem, int nblocks, cudaStream_t st);
+cudaError_t launch_k4_wtab(const DevSys& S, const DevIfc& F, const TcPlan* plan_dev, int ksteps, uint16_t* wtab,
+                           cudaStream_t st);
 // fp4_bte.cu: iteration0 and TConduct on device-resident arrays (reference layouts)
 cudaError_t launch_iteration0(int nb, int nptk, int nlist, int nsr, const int* nequi, const int* allequi,
                               const double* energy, const double* velocity, const double* tau_zero, double* F,

@@ -22,8 +22,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fp4_device.cuh"
 #include "fp4_internal.h"
+#include "fp4_tc.cuh"
 
 namespace fp4 {
 
@@ -85,7 +88,7 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15
 constexpr size_t kAllZCap = 72 * 1024;
 
 __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
-                                              int allz, int njjl) {
+                                              int allz, int njjl, bool noz = false) {
     Layout L;
     L.allz = allz;
     L.njjl = njjl;
@@ -93,7 +96,7 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     const size_t nb2 = (size_t)nb * nb;
     size_t o = 0;
     L.z = o;
-    o = al16(o + ((kind >= 2) ? (allz ? nb2 : (size_t)nb) * npi * 9 * cs : 0));
+    o = al16(o + ((kind >= 2 && !noz) ? (allz ? nb2 : (size_t)nb) * npi * 9 * cs : 0));
     L.kap = o;
     o = al16(o + ((kind >= 2) ? (size_t)ntri * 16 : 0));
     L.pt = o;
@@ -149,6 +152,41 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
     Layout B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, nl);
     if (nl && B.total > kAllZCap) B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, 0);
     return B;
+}
+
+// Shared memory of the tensor-core contraction, after the common layout (no Z
+// tables): the A tiles of the two warpgroups, the B tables and FP64 Z entries
+// of one group of bins, two mbarriers, the TMEM address and the parities of the
+// two mbarriers, the group's bins and its chunk list.
+struct TcLayout {
+    size_t a, b, zs, bar, slot, gbin, chunk, total;
+};
+
+__host__ __device__ inline Layout k4_layout_tcbase(int NT, int nb, int npi, int ntri, int lsum, int nptk) {
+    const int nl = nptk <= kMaxJJList ? nptk : 0;
+    return k4_layout_z(2, NT, true, nb, npi, ntri, lsum, 0, nl, true);
+}
+
+__host__ __device__ inline TcLayout k4_tc_layout(size_t base, int ksteps, int bin_bytes, int zbins, int npi,
+                                                 int chunk_cap) {
+    TcLayout T;
+    size_t o = (base + 127) & ~(size_t)127;
+    T.a = o;
+    o += 2 * (size_t)ksteps * kTcRows * 32;
+    T.b = o;
+    o += (size_t)zbins * bin_bytes;
+    T.zs = o;
+    o += (size_t)zbins * npi * 9 * 16;
+    T.bar = o;
+    o += 16;
+    T.slot = o;
+    o += 16;
+    T.gbin = o;
+    o = al16(o + (size_t)zbins * 4);
+    T.chunk = o;
+    o = al16(o + (size_t)chunk_cap * 4);
+    T.total = o;
+    return T;
 }
 
 template <bool MIXED>
@@ -469,15 +507,284 @@ __device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Lay
     __syncthreads();
 }
 
-template <int NT, bool MIXED, bool LIST>
+// ---------------------------------------------------------------------------- tensor-core phase B
+// One value of a bin's B table: the (n, k) entry of pass `pass`, where n runs over
+// the pass's blocks (32 columns each: re(Z[sr]) at sr, im(Z[sr]) at 9+sr) and k over
+// its classes (6 values each, see TcPlan).  Zero outside the class's own block.
+__device__ __forceinline__ uint16_t tc_b_value(const TcPlan* P, const double2* Zs, int npi, int slot, int pass,
+                                               int n, int k) {
+    const int lb = n >> 5, nn = n & 31;
+    if (nn >= 18) return 0;
+    const int4 bk = P->blk[P->pass_blk0[pass] + lb];
+    const int cls = P->pass_cls0[pass] + k / 6;
+    if (cls < bk.x || cls >= bk.y) return 0;
+    const int r6 = k - (k / 6) * 6, split = r6 >> 1, ri = r6 & 1;
+    const int ro = nn >= 9, sr = nn - 9 * ro;
+    const double2 z = Zs[((size_t)slot * npi + cls) * 9 + sr];
+    // the product's real (ro = 0) or imaginary (ro = 1) part takes, from A's
+    // (re, im) pair of w: (Z.re, -Z.im) or (Z.im, Z.re)
+    const double v = (ri == 0) ? (ro == 0 ? z.x : z.y) : (ro == 0 ? -z.y : z.x);
+    uint16_t hi, lo;
+    tc::split_bf16(v, hi, lo);
+    return split == 1 ? lo : hi;
+}
+
+// Phase B on the tensor cores (mixed precision, RTA): the queued processes of
+// each (i,j) bin are contracted 128 at a time.  Row m of the A tile holds the
+// bf16 hi/lo Bloch phases w_p(q'') of process m (a copy of its q'' row of the
+// phase table); the bin's B table holds the bf16 hi/lo split of
+// Z_p^{(ij)}[s][r], block-diagonal over the atom-pair blocks.  One product per
+// pass gives, in TMEM, T_b[s][r] = sum_{p in b} w_p Z_p[s][r] for every block b
+// of the pass, and the epilogue forms V = sum_b u_b^T T_b v_b with u_b the
+// eigenvector of the third phonon on atom a3 of block b (conjugated for the +-
+// and -- channels) and v_b the conjugated eigenvector of the fourth on atom a4.
+// Each warpgroup owns one A tile, one mbarrier and one 128-column TMEM region
+// and takes every other chunk of the group's bins.  The Bose/Gaussian weights
+// are computed in FP64 while the product runs.
+template <int NT>
+__device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layout& L, const TcLayout& TL,
+                              const unsigned long long* qbase, const double* qsig, int ch, int ii, int q0,
+                              unsigned long long& my_contr) {
+    const DevSys& S = p.S;
+    const DevIfc& F = p.F;
+    const TcPlan* P = p.tc;
+    const int nb = S.nb, nb2 = nb * nb, npi = F.npi;
+    const double2* kap = reinterpret_cast<const double2*>(smem + L.kap);
+    double* racc = reinterpret_cast<double*>(smem + L.racc);
+    double* wacc = reinterpret_cast<double*>(smem + L.wacc);
+    int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+    unsigned char* Abuf = smem + TL.a;
+    unsigned char* Bbuf = smem + TL.b;
+    double2* Zs = reinterpret_cast<double2*>(smem + TL.zs);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TL.bar);
+    uint32_t* slotw = reinterpret_cast<uint32_t*>(smem + TL.slot);  // [0] TMEM base, [1+g] parity of mbarrier g
+    int* gbin = reinterpret_cast<int*>(smem + TL.gbin);
+    int* chunks = reinterpret_cast<int*>(smem + TL.chunk);
+    const int zbins = P->zbins, npass = P->npass, ksteps = P->ksteps, bin_bytes = P->bin_bytes;
+    const int wg = threadIdx.x >> 7, m = threadIdx.x & 127, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tbase = slotw[0];
+    const uint32_t tregion = tbase + (uint32_t)(wg * kTcRegionCols) + ((uint32_t)((warp & 3) * 32) << 16);
+    uint32_t par = slotw[1 + wg];
+    const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;
+    const uint4* wrows = reinterpret_cast<const uint4*>(p.wtab + (size_t)(ch != 0) * S.nptk * ksteps * 16);
+    unsigned char* Aw = Abuf + (size_t)wg * ksteps * kTcRows * 32;
+    const double sqrtpi = sqrt(3.141592653589793238);
+    const double floor_sigma = (double)0.001f;
+    constexpr int WS = wb_stride(NT);
+    if (threadIdx.x == 0) misc[4] = 0;
+    __syncthreads();
+    for (;;) {
+        // the next group: up to zbins non-empty bins and their chunks of kTcRows processes
+        if (threadIdx.x == 0) {
+            int b = misc[4], ng = 0, nc = 0;
+            while (b < nb2 && ng < zbins) {
+                const int n = min(cnt[b], p.subcap);
+                if (n > 0) {
+                    gbin[ng] = b;
+                    for (int e = 0; e < n; e += kTcRows) chunks[nc++] = (ng << 16) | (e / kTcRows);
+                    ng++;
+                }
+                b++;
+            }
+            misc[4] = b;
+            misc[5] = ng;
+            misc[6] = nc;
+            if (ng) atomicAdd(&p.stats[5], (unsigned long long)ng);
+        }
+        __syncthreads();
+        const int ng = misc[5], nc = misc[6];
+        if (ng == 0 || misc[7]) break;
+        // FP64 reciprocal cluster entries of the group's bins
+        for (int idx = threadIdx.x; idx < ng * npi * 9; idx += blockDim.x) {
+            const int slot = idx / (npi * 9), rem = idx - slot * (npi * 9), pc = rem / 9, sr = rem - pc * 9;
+            const int bin = gbin[slot], i = bin / nb, j = bin - i * nb;
+            Zs[idx] = k4_z_entry(S, F, kap, ch, q0, ii, i, j, pc, sr);
+        }
+        __syncthreads();
+        // their B tables, 16 bytes (8 values of one row n) per store
+        const int chunks16 = bin_bytes >> 4;
+        for (int idx = threadIdx.x; idx < ng * chunks16; idx += blockDim.x) {
+            const int slot = idx / chunks16;
+            const int off = (idx - slot * chunks16) << 4;
+            int pass = 0;
+            while (pass + 1 < npass && P->pass_boff[pass + 1] <= off) pass++;
+            const int rel = off - P->pass_boff[pass];
+            const int N = 32 * (P->pass_blk0[pass + 1] - P->pass_blk0[pass]);
+            const int s = rel / (N * 32), within = rel - s * (N * 32);
+            const int n = (within >> 8) * 8 + ((within >> 4) & 7);
+            const int kb = s * 16 + ((within >> 7) & 1) * 8;
+            uint32_t w4[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                const uint32_t v0 = tc_b_value(P, Zs, npi, slot, pass, n, kb + 2 * x);
+                const uint32_t v1 = tc_b_value(P, Zs, npi, slot, pass, n, kb + 2 * x + 1);
+                w4[x] = v0 | (v1 << 16);
+            }
+            *reinterpret_cast<uint4*>(Bbuf + (size_t)slot * bin_bytes + off) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        // the chunks: warpgroup wg takes chunks wg, wg+2, ...
+        for (int c = wg; c < nc; c += 2) {
+            const int code = chunks[c];
+            const int slot = code >> 16, e0 = (code & 0xffff) * kTcRows;
+            const int bin = gbin[slot], i = bin / nb, j = bin - i * nb;
+            const int n = min(cnt[bin], p.subcap) - e0;
+            const bool valid = m < n;
+            int a = 0, b = 0, cc = 0, ss = 0, k = 0, l = 0, jj = 0;
+            double sig = 0.0;
+            if (valid) {
+                const size_t qi = (size_t)bin * p.subcap + e0 + m;
+                unpack_proc(qbase[qi], a, b, cc, ss, k, l);
+                sig = qsig[qi];
+                jj = q_index(S, a, b, cc);
+                // A row m: the phase row of q''
+                const uint4* src = wrows + (size_t)jj * ksteps * 2;
+                for (int x = 0; x < 2 * ksteps; x++)
+                    *reinterpret_cast<uint4*>(Aw + (size_t)(x >> 1) * (kTcRows * 32) + tc::kmajor_offset(m, (x & 1) * 8)) =
+                        __ldg(src + x);
+            }
+            tc::fence_async_smem();
+            tc::fence_before_sync();
+            tc::named_sync(1 + wg, kTcRows);
+            double wts[NT];
+#pragma unroll
+            for (int t = 0; t < NT; t++) wts[t] = 0.0;
+            float2 V = make_float2(0.f, 0.f);
+            bool ok = true;
+            for (int pass = 0; pass < npass; pass++) {
+                if (m == 0) {
+                    tc::fence_after_sync();
+                    const int N = 32 * (P->pass_blk0[pass + 1] - P->pass_blk0[pass]);
+                    const uint32_t idesc = tc::idesc_bf16_f32(N);
+                    const int ks0 = P->pass_kstep0[pass], ksn = P->pass_kstep0[pass + 1] - ks0;
+                    const uint32_t aaddr = tc::smem_u32(Aw) + (uint32_t)ks0 * (kTcRows * 32);
+                    const uint32_t baddr = tc::smem_u32(Bbuf + (size_t)slot * bin_bytes + P->pass_boff[pass]);
+                    for (int x = 0; x < ksn; x++)
+                        tc::mma_bf16(tbase + (uint32_t)(wg * kTcRegionCols), tc::smem_desc(aaddr + x * (kTcRows * 32)),
+                                     tc::smem_desc(baddr + x * N * 32), idesc, x > 0);
+                    tc::commit(tc::smem_u32(&bars[wg]));
+                    atomicAdd(&p.stats[6], (unsigned long long)(ksn * (N / 16)));
+                }
+                if (pass == 0 && valid) {
+                    // FP64 weights of every temperature, while the product runs
+                    const double* x1 = p.wb + (size_t)(ii * nb + j) * WS;
+                    const double* x2 = p.wb + (size_t)(jj * nb + k) * WS;
+                    const double* x3 = p.wb + (size_t)(ss * nb + l) * WS;
+                    const double omega = wvw[4 * (q0 * nb + i)];
+                    const double w1 = x1[0], w2 = x2[0], w3 = x3[0];
+                    const double sv = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
+                    const double delta =
+                        (ch == 0) ? __dadd_rn(__dadd_rn(sv, w2), -w3) : __dadd_rn(__dadd_rn(sv, -w2), -w3);
+                    if (sig <= floor_sigma) sig = 1.0 / sqrtpi;
+                    const double g = exp(-(delta * delta) / (sig * sig));
+                    const double base = g / (sig * sqrtpi * (omega * w1 * w2 * w3));
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        if (t < p.nT) {
+                            const double f1 = x1[1 + t], f2 = x2[1 + t], f3 = x3[1 + t];
+                            double bc;
+                            if (ch == 0)
+                                bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
+                            else if (ch == 1)
+                                bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
+                            else
+                                bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
+                            wts[t] = bc * base;
+                        }
+                    }
+                }
+                const bool done = tc::mbar_wait(tc::smem_u32(&bars[wg]), par);
+                ok = tc::named_all(1 + wg, kTcRows, done);
+                if (!ok) break;  // par stays the parity of the product still pending
+                par ^= 1u;
+                tc::fence_after_sync();
+                const float2* e2 = S.eigf + (size_t)(jj * nb + k) * nb;
+                const float2* e3 = S.eigf + (size_t)(ss * nb + l) * nb;
+                for (int bl = P->pass_blk0[pass]; bl < P->pass_blk0[pass + 1]; bl++) {
+                    const uint32_t col = (uint32_t)((bl - P->pass_blk0[pass]) * 32);
+                    float T0[16], T1[16];
+                    tc::ld16(tregion + col, T0);
+                    tc::ld16(tregion + col + 16, T1);
+                    tc::ld_wait();
+                    if (valid) {
+                        const int4 bk = P->blk[bl];
+                        float2 u[3], v[3];
+#pragma unroll
+                        for (int x = 0; x < 3; x++) {
+                            u[x] = e2[3 * bk.z + x];
+                            if (ch != 0) u[x] = cconjf(u[x]);
+                            v[x] = cconjf(e3[3 * bk.w + x]);
+                        }
+                        float2 tt = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int x = 0; x < 3; x++) {
+                            float2 h = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int r = 0; r < 3; r++) {
+                                const int sr = x * 3 + r;
+                                const float im = (sr < 7) ? T0[9 + sr] : T1[sr - 7];
+                                h = cmacf(h, make_float2(T0[sr], im), v[r]);
+                            }
+                            tt = cmacf(tt, u[x], h);
+                        }
+                        V.x += tt.x;
+                        V.y += tt.y;
+                    }
+                }
+                tc::fence_before_sync();
+                if (pass + 1 < npass) tc::named_sync(1 + wg, kTcRows);
+            }
+            if (!ok) {
+                if (m == 0) {
+                    atomicOr(p.err, kErrTimeout);
+                    misc[7] = 1;
+                }
+                break;
+            }
+            double accr[NT], accw[NT];
+            const double v2 = (double)V.x * (double)V.x + (double)V.y * (double)V.y;
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                accr[t] = valid ? wts[t] * v2 : 0.0;
+                accw[t] = valid ? wts[t] : 0.0;
+            }
+            if (valid) my_contr++;
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                for (int o = 16; o > 0; o >>= 1) {
+                    accr[t] += __shfl_down_sync(0xffffffffu, accr[t], o);
+                    accw[t] += __shfl_down_sync(0xffffffffu, accw[t], o);
+                }
+                if (lane == 0 && t < p.nT) {
+                    atomicAdd(&racc[i * NT + t], accr[t]);
+                    atomicAdd(&wacc[i * NT + t], accw[t]);
+                }
+            }
+        }
+        if (m == 0) slotw[1 + wg] = par;
+        __syncthreads();
+    }
+    for (int x = threadIdx.x; x < nb2; x += blockDim.x) cnt[x] = 0;
+    __syncthreads();
+}
+
+template <int NT, bool MIXED, bool LIST, bool TC>
 __device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem, const Layout& L,
                                          const unsigned long long* qbase, const double* qsig, const long long* qpos,
                                          int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
                                          unsigned long long& my_contr) {
-    if (L.allz)
+    if constexpr (TC) {
+        const TcPlan* P = p.tc;
+        const Layout Lb = k4_layout_tcbase(NT, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
+        const TcLayout TL = k4_tc_layout(Lb.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap);
+        k4_phase_b_tc<NT>(p, smem, L, TL, qbase, qsig, ch, ii, q0, my_contr);
+    } else if (L.allz) {
         k4_phase_b_all<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
-    else
+    } else {
         k4_phase_b<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+    }
 }
 
 // True (for the whole CTA) when some (i,j) queue could overflow within the next
@@ -543,7 +850,7 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
     int iter = 0;
     for (long long base = 0; base < total; base += blockDim.x, iter++) {
         if ((iter % kCheckEvery) == 0 && queue_nearly_full(p, cnt, nb2, misc))
-            k4_flush<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+            k4_flush<NT, MIXED, true, false>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
         const long long e = base + threadIdx.x;
         if (e >= total) continue;
         int i = 0;
@@ -586,7 +893,7 @@ __device__ void k4_list_segment(const P4Params& p, unsigned char* smem, const La
         qpos[qi] = pos;
     }
     __syncthreads();
-    k4_flush<NT, MIXED, true>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+    k4_flush<NT, MIXED, true, false>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
 }
 
 // Per-thread work counters of one kernel, flushed into a P4Params::stats array.
@@ -681,8 +988,9 @@ __device__ void k4_cta_init(const P4Params& p, unsigned char* smem, const Layout
 
 }
 
-// One work item (q = List(ll), q', channel) of one solve.
-template <int KIND, int NT, bool MIXED>
+// One work item (q = List(ll), q', channel) of one solve.  TC: phase B on the
+// tensor cores (RTA, mixed precision).
+template <int KIND, int NT, bool MIXED, bool TC = false>
 __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, const Layout& L, int wi,
                                         unsigned long long* qbase, double* qsig, long long* qpos, K4Stats& st) {
     const DevSys& S = p.S;
@@ -783,7 +1091,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         for (int base = 0; base < total; base += blockDim.x, iter++) {
             if (KIND == 2 && (iter % kCheckEvery) == 0) {
                 if (queue_nearly_full(p, cnt, nb2, misc))
-                    k4_flush<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+                    k4_flush<NT, MIXED, LIST, TC>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                                 my_contr);
             }
             if (base + (int)threadIdx.x < total) {
@@ -859,7 +1167,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         }
         if (KIND == 2) {
             __syncthreads();
-            k4_flush<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
+            k4_flush<NT, MIXED, LIST, TC>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                         my_contr);
         }
     }
@@ -906,6 +1214,94 @@ __global__ void __launch_bounds__(kThreads, (ctas_per_sm<KIND, NT, MIXED>())) k4
         k4_item<KIND, NT, MIXED>(p, smem, L, wi, qbase, qsig, qpos, st);
     }
     k4_flush_stats(p.stats, st, reinterpret_cast<double*>(smem + L.red));
+}
+
+// The four-phonon RTA work kernel with phase B on the tensor cores (mixed
+// precision): phase A as in k4_work, then k4_phase_b_tc.  Each CTA holds 256
+// TMEM columns (two warpgroup regions) for its lifetime; two CTAs per SM use
+// the whole TMEM.  A bounded wait that gives up raises kErrTimeout and stops
+// the CTA, which waits (bounded) for its outstanding products before it frees
+// its TMEM.
+template <int NT>
+__global__ void __launch_bounds__(kThreads, 2) k4_work_tc(P4Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nb2 = p.S.nb * p.S.nb;
+    const TcPlan* P = p.tc;
+    const Layout L = k4_layout_tcbase(NT, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
+    const TcLayout TL = k4_tc_layout(L.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap);
+    int* misc = reinterpret_cast<int*>(smem + L.misc);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TL.bar);
+    uint32_t* slotw = reinterpret_cast<uint32_t*>(smem + TL.slot);
+    k4_cta_init<2, true>(p, smem, L);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(tc::smem_u32(&bars[0]), 1);
+        tc::mbar_init(tc::smem_u32(&bars[1]), 1);
+        tc::mbar_fence_init();
+        slotw[1] = 0;
+        slotw[2] = 0;
+        misc[7] = 0;
+    }
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(tc::smem_u32(&slotw[0]), 2 * kTcRegionCols);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    unsigned long long* qbase = p.queue + (size_t)blockIdx.x * nb2 * p.subcap;
+    double* qsig = p.queue_sigma + (size_t)blockIdx.x * nb2 * p.subcap;
+    K4Stats st{0, 0, 0, 0};
+    for (;;) {
+        if (threadIdx.x == 0) misc[0] = atomicAdd(p.work_counter, 1);
+        __syncthreads();
+        const int wi = misc[0];
+        if (wi >= p.nwork || misc[7]) break;
+        k4_item<2, NT, true, true>(p, smem, L, wi, qbase, qsig, nullptr, st);
+    }
+    k4_flush_stats(p.stats, st, reinterpret_cast<double*>(smem + L.red));
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0 && misc[7]) {
+        // after a wait that gave up: give the products still in flight a bounded time
+        tc::mbar_wait(tc::smem_u32(&bars[0]), slotw[1]);
+        tc::mbar_wait(tc::smem_u32(&bars[1]), slotw[2]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(slotw[0], 2 * kTcRegionCols);
+}
+
+// A rows of the tensor-core contraction for every q'' and both channel signs:
+// 16-byte words of 8 bf16 values, the K layout of TcPlan with the Bloch phases
+// w_p(q'') = exp(+-2 pi i n''.D_p / N) formed in FP64 from the exact root tables.
+__global__ void k4_wtab(DevSys S, DevIfc F, const TcPlan* P, int ksteps, uint16_t* wtab) {
+    const int words = 2 * ksteps;  // 16-byte words per row
+    const size_t total = (size_t)2 * S.nptk * words;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        const int word = (int)(x % words);
+        const size_t row = x / words;
+        const int q = (int)(row % S.nptk), sgn = (int)(row / S.nptk);
+        int a, b, c;
+        q_coords(S, q, a, b, c);
+        const int k0 = word * 8;
+        int pass = 0;
+        while (pass + 1 < P->npass && P->pass_kstep0[pass + 1] * 16 <= k0) pass++;
+        uint32_t w4[4] = {0, 0, 0, 0};
+        for (int y = 0; y < 8; y++) {
+            const int kk = k0 + y - P->pass_kstep0[pass] * 16;
+            const int cls = P->pass_cls0[pass] + kk / 6;
+            if (cls >= P->pass_cls0[pass + 1]) continue;
+            const int r6 = kk - (kk / 6) * 6, split = r6 >> 1, ri = r6 & 1;
+            const int4 D = F.pi_d[cls];
+            double2 w = lattice_phase(S, a, b, c, D.x, D.y, D.z);
+            if (sgn) w = cconj(w);
+            uint16_t hi, lo;
+            tc::split_bf16(ri ? w.y : w.x, hi, lo);
+            const uint32_t v = (split == 2) ? lo : hi;
+            w4[y >> 1] |= v << (16 * (y & 1));
+        }
+        reinterpret_cast<uint4*>(wtab)[x] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
 }
 
 // Several solves in one persistent launch (the serving path).  The tick lists
@@ -1011,6 +1407,74 @@ size_t k4_smem(int kind, int nT, bool mixed, const DevSys& S, const DevIfc& F) {
 }
 
 int k4_threads() { return kThreads; }
+
+int k4_tc_plan(int nb, int natoms, int npi, const int* blk_start, int subcap, TcPlan& P) {
+    P = TcPlan{};
+    const int nat2 = natoms * natoms;
+    for (int b = 0; b < nat2; b++)
+        if (blk_start[b] < blk_start[b + 1]) {
+            if (P.nblk >= kTcMaxBlocks) return -1;
+            P.blk[P.nblk++] = make_int4(blk_start[b], blk_start[b + 1], b / natoms, b % natoms);
+        }
+    if (P.nblk == 0 || blk_start[nat2] != npi) return -1;
+    int ks = 0, boff = 0;
+    for (int b0 = 0; b0 < P.nblk; b0 += kTcPassBlocks) {
+        const int b1 = std::min(P.nblk, b0 + kTcPassBlocks);
+        const int x = P.npass++;
+        P.pass_blk0[x] = b0;
+        P.pass_cls0[x] = P.blk[b0].x;
+        P.pass_kstep0[x] = ks;
+        P.pass_boff[x] = boff;
+        const int C = P.blk[b1 - 1].y - P.blk[b0].x;
+        const int k = (6 * C + 15) / 16;
+        ks += k;
+        boff += k * 32 * (b1 - b0) * 32;  // K-steps x N rows x 32 bytes
+    }
+    P.pass_blk0[P.npass] = P.nblk;
+    P.pass_cls0[P.npass] = npi;
+    P.pass_kstep0[P.npass] = ks;
+    P.pass_boff[P.npass] = boff;
+    P.ksteps = ks;
+    P.bin_bytes = boff;
+    P.zbins = 1;
+    P.chunk_cap = (subcap + kTcRows - 1) / kTcRows;
+    (void)nb;
+    return 0;
+}
+
+// Shared memory of k4_work_tc for the plan's zbins (the plan's chunk_cap must match).
+size_t k4_tc_smem(int nT, const DevSys& S, const DevIfc& F, const TcPlan& P) {
+    const Layout L = k4_layout_tcbase(round_nt(nT), S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], S.nptk);
+    return k4_tc_layout(L.total, P.ksteps, P.bin_bytes, P.zbins, F.npi, P.chunk_cap).total;
+}
+
+int k4_tc_ctas_per_sm() { return 2; }
+
+cudaError_t launch_k4_tc(int nT, const P4Params& p, size_t smem, int nblocks, cudaStream_t st) {
+    const int NT = round_nt(nT);
+#define FP4_K4TC(NTV)                                                                                            \
+    if (NT == NTV) {                                                                                             \
+        cudaError_t e = cudaFuncSetAttribute(k4_work_tc<NTV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (e != cudaSuccess) return e;                                                                          \
+        k4_work_tc<NTV><<<nblocks, kThreads, smem, st>>>(p);                                                     \
+        return cudaGetLastError();                                                                               \
+    }
+    FP4_K4TC(1)
+    FP4_K4TC(2)
+    FP4_K4TC(4)
+    FP4_K4TC(8)
+#undef FP4_K4TC
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_k4_wtab(const DevSys& S, const DevIfc& F, const TcPlan* plan_dev, int ksteps, uint16_t* wtab,
+                           cudaStream_t st) {
+    const size_t total = (size_t)2 * S.nptk * 2 * ksteps;
+    const int threads = 256;
+    const int blocks = (int)std::min<size_t>((total + threads - 1) / threads, 148 * 16);
+    k4_wtab<<<blocks, threads, 0, st>>>(S, F, plan_dev, ksteps, wtab);
+    return cudaGetLastError();
+}
 int k4_round_nt(int nT) { return round_nt(nT); }
 int k4_multi_ctas_per_sm() { return kMultiCtasPerSm; }
 

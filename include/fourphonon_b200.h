@@ -41,7 +41,8 @@ extern "C" {
 #define FP4_E_STATE (-5)    /* call order (e.g. no system set) */
 
 #define FP4_PREC_FP64 0  /* all-FP64 drop-in */
-#define FP4_PREC_MIXED 1 /* FP32 contraction, FP64 filter/weights/reductions */
+#define FP4_PREC_MIXED 1 /* split-bf16 tensor-core contraction (FP32 accumulate), FP64 filter/weights/reductions */
+#define FP4_PREC_MIXED_SIMT 2 /* FP32 contraction on the CUDA cores, FP64 filter/weights/reductions */
 
 typedef struct fp4_ctx fp4_ctx;
 
@@ -64,7 +65,13 @@ typedef struct {
 int fp4_create(fp4_ctx **ctx, int device);
 int fp4_destroy(fp4_ctx *ctx);
 const char *fp4_last_error(const fp4_ctx *ctx);
-/* FP4_PREC_FP64 (default) or FP4_PREC_MIXED for the rate drivers. */
+/*
+ * FP4_PREC_FP64 (default), FP4_PREC_MIXED or FP4_PREC_MIXED_SIMT for the rate
+ * drivers.  FP4_PREC_MIXED runs the four-phonon RTA contraction on the tensor
+ * cores (split bf16 operands, FP32 accumulation) when its tables fit in
+ * shared memory, else as FP4_PREC_MIXED_SIMT; the other mixed drivers use
+ * the FP32 CUDA-core contraction.  Filters, weights and sums stay FP64.
+ */
 int fp4_set_precision(fp4_ctx *ctx, int precision);
 
 /*
@@ -366,10 +373,24 @@ int fp4_rta4_partials(fp4_ctx *ctx, int32_t ll, int32_t ii0, int32_t ii1, int32_
                       double *rate_pm, double *rate_mm, double *wp_pp, double *wp_pm, double *wp_mm);
 
 /*
+ * Self-check of the tensor-core path (no counterpart in the reference): on
+ * the current device, D(128,N) = A(128,K) * B(N,K)^T with bf16 A and B
+ * (row-major host arrays of raw bf16 bits) and FP32 accumulation, through the
+ * same shared-memory layout, tcgen05.mma, mbarrier and TMEM read-back that the
+ * mixed-precision four-phonon contraction uses.  K a multiple of 16 up to
+ * 1024, N a multiple of 16 in [16, 256]; D is a row-major host array.
+ */
+int fp4_tc_selftest(int32_t K, int32_t N, const uint16_t *A, const uint16_t *B, float *D);
+
+/*
  * Work counters of the last four-phonon call: [0] surviving processes,
  * [1] contracted processes, [2] broadening evaluations (one per (q'',k,l)
  * candidate triple), [3] energy tests in the sorted windows, [4] reciprocal
- * cluster tables built, [5..7] reserved (0).
+ * cluster tables built on the CUDA cores (one per branch i, or per work item
+ * when all branches are built at once), [5] (i,j) tables built for the
+ * tensor cores, [6] tensor-core work in units of one 128 x 16 x 16 product
+ * (a tcgen05.mma K-step of N columns counts N/16; 65,536 flops per unit),
+ * [7] 1 if the contraction ran on the tensor cores, else 0.
  */
 int fp4_last_counters(const fp4_ctx *ctx, int64_t counters[8]);
 

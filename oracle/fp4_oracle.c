@@ -704,6 +704,32 @@ void fp4o_rta4_range(const fp4o_sys *s, const fp4o_ifc *f, int mm0, int mm1, int
 }
 
 /*
+ * Timing sample of RTA_driver_4ph spread over the whole workload: the listed
+ * modes (0-based), each over the q' points ii_offset, ii_offset + ii_stride,
+ * ... (0-based), all three channels.  Returns the number of surviving
+ * processes visited; the rates are discarded (timing use only).
+ */
+int64_t fp4o_rta4_strided(const fp4o_sys *s, const fp4o_ifc *f, const int32_t *modes, int nmodes, int ii_stride,
+                          int ii_offset) {
+    const int nq = (s->nptk - ii_offset + ii_stride - 1) / ii_stride;
+    int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
+    for (int x = 0; x < nmodes * nq; x++) {
+        const int mm = modes[x / nq] + 1, ii = ii_offset + (x % nq) * ii_stride;
+        if (!gate(s, mm)) continue;
+        for (int ch = 0; ch < 3; ch++) {
+            acc4_t a;
+            memset(&a, 0, sizeof a);
+            a.ii0 = ii;
+            a.ii1 = ii + 1;
+            proc4_one(s, f, mm, ch, 2, &a);
+            total += a.n;
+        }
+    }
+    return total;
+}
+
+/*
  * Bounded sample of RTA_driver_4ph for timing: modes [mm0,mm1), each
  * restricted to the q' range [ii0,ii1).  Returns the number of surviving
  * processes visited; rates are not normalised (timing use only).

@@ -45,6 +45,7 @@ def lib():
         _lib.fp4o_ind_only4.restype = ct.c_int64
         _lib.fp4o_num_threads.restype = ct.c_int
         _lib.fp4o_rta4_sample.restype = ct.c_int64
+        _lib.fp4o_rta4_strided.restype = ct.c_int64
     return _lib
 
 
@@ -151,6 +152,14 @@ class Oracle:
         out = [np.zeros(nm) for _ in range(6)]
         lib().fp4o_rta4_range(ct.byref(self.sys), ct.byref(self.ifc4), mm0, mm1, ii0, ii1, *[_p(x) for x in out])
         return out
+
+    def rta4_strided(self, modes, ii_stride, ii_offset=0):
+        """Timing sample: RTA_driver_4ph work of the listed modes (0-based) over the
+        q' points ii_offset, ii_offset + ii_stride, ...; returns the surviving
+        processes visited."""
+        m = np.ascontiguousarray(modes, dtype=np.int32)
+        return int(lib().fp4o_rta4_strided(ct.byref(self.sys), ct.byref(self.ifc4), _p(m), int(m.size),
+                                             int(ii_stride), int(ii_offset)))
 
     def rta4_sample(self, mm0, mm1, ii0, ii1):
         """Timing sample: RTA_driver_4ph work for modes [mm0,mm1) restricted to

@@ -185,9 +185,10 @@ def _rta_kappa(s, rate_total, tconduct):
     return np.trace(k) / 3.0
 
 
-def test_mixed_path_kappa_within_1e_4(s6):
+@pytest.mark.parametrize("precision", [abi.FP4_PREC_MIXED, abi.FP4_PREC_MIXED_SIMT])
+def test_mixed_path_kappa_within_1e_4(s6, precision):
     c64 = abi.Context(0, abi.FP4_PREC_FP64)
-    cmx = abi.Context(0, abi.FP4_PREC_MIXED)
+    cmx = abi.Context(0, precision)
     try:
         r64 = c64.rta_driver_4ph(s6)
         rmx = cmx.rta_driver_4ph(s6)

@@ -52,6 +52,21 @@ def cmx():
     c.close()
 
 
+@pytest.fixture(scope="module")
+def csimt():
+    c = abi.Context(0, abi.FP4_PREC_MIXED_SIMT)
+    yield c
+    c.close()
+
+
+MIXED_MODES = [abi.FP4_PREC_MIXED, abi.FP4_PREC_MIXED_SIMT]
+ALL_MODES = [abi.FP4_PREC_FP64] + MIXED_MODES
+
+
+def pick(precision, c64, cmx, csimt):
+    return {abi.FP4_PREC_FP64: c64, abi.FP4_PREC_MIXED: cmx, abi.FP4_PREC_MIXED_SIMT: csimt}[precision]
+
+
 # ---------------------------------------------------------------------------- 12 branches, per-branch tables
 
 
@@ -71,9 +86,11 @@ def test_layered_rta4_fp64(c64, layered):
         assert ok, (name, e)
 
 
-def test_layered_rta4_mixed(cmx, layered):
+@pytest.mark.parametrize("precision", MIXED_MODES)
+def test_layered_rta4_mixed(cmx, csimt, layered, precision):
     s, mm0, mm1, o = layered
-    g = cmx.rta_driver_4ph(s)
+    ctx = cmx if precision == abi.FP4_PREC_MIXED else csimt
+    g = ctx.rta_driver_4ph(s)
     errs = {}
     for x, name in enumerate(CH):
         ok, e = close(g[name][0][mm0:mm1], o[x][mm0:mm1], RTOL_MIXED_RATE)
@@ -82,17 +99,17 @@ def test_layered_rta4_mixed(cmx, layered):
     for x, name in enumerate(WP):  # the weights stay FP64 in the mixed path
         ok, e = close(g[name][0][mm0:mm1], o[3 + x][mm0:mm1], RTOL_FP64)
         assert ok, (name, e)
-    print("layered mixed per-mode rate error vs oracle:", errs)
+    print("layered mixed per-mode rate error vs oracle:", precision, errs, "tensor cores:", ctx.counters()[7])
 
 
 # ---------------------------------------------------------------------------- four fused temperatures
 
 
-@pytest.mark.parametrize("precision", [abi.FP4_PREC_FP64, abi.FP4_PREC_MIXED])
-def test_four_temperatures_fused(c64, cmx, precision):
+@pytest.mark.parametrize("precision", ALL_MODES)
+def test_four_temperatures_fused(c64, cmx, csimt, precision):
     temps = (100.0, 300.0, 500.0, 1000.0)
     s = H.cached_solve("zincblende", (4, 4, 4), temperatures=temps)
-    ctx = c64 if precision == abi.FP4_PREC_FP64 else cmx
+    ctx = pick(precision, c64, cmx, csimt)
     g = ctx.rta_driver_4ph(s)
     rtol = RTOL_FP64 if precision == abi.FP4_PREC_FP64 else RTOL_MIXED_RATE
     for t, T in enumerate(temps):
@@ -171,10 +188,10 @@ def grid16():
     return s, ll, ii0, ii1, mm0, mm1, ref
 
 
-@pytest.mark.parametrize("precision", [abi.FP4_PREC_FP64, abi.FP4_PREC_MIXED])
-def test_grid16_partials(c64, cmx, grid16, precision):
+@pytest.mark.parametrize("precision", ALL_MODES)
+def test_grid16_partials(c64, cmx, csimt, grid16, precision):
     s, ll, ii0, ii1, mm0, mm1, ref = grid16
-    ctx = c64 if precision == abi.FP4_PREC_FP64 else cmx
+    ctx = pick(precision, c64, cmx, csimt)
     full = ctx.rta_driver_4ph(s)
     rtol = RTOL_FP64 if precision == abi.FP4_PREC_FP64 else RTOL_MIXED_RATE
     errs = []
@@ -194,4 +211,4 @@ def test_grid16_partials(c64, cmx, grid16, precision):
         for name in CH + WP:
             ok, e = close(tot[name], full[name][t][mm0:mm1], 1e-12)
             assert ok, (t, name, e)
-    print("16^3 partial-sum rate error vs oracle:", max(errs))
+    print("16^3 partial-sum rate error vs oracle:", precision, max(errs))
