@@ -338,8 +338,10 @@ def time_steps(torch, ctx, s, steps, flush):
         e1.record()
         torch.cuda.synchronize()
         nproc, ncontr, call_ms, kms, launches = ctx.stats()
+        item, phb = ctx.phase_cycles()
+        phases = {"phase_a_frac": (item - phb) / item if item else None, "phase_b_frac": phb / item if item else None}
         out.append(dict(ms=e0.elapsed_time(e1), kms=kms, nproc=nproc, ncontr=ncontr, launches=launches,
-                        counters=ctx.counters(), rates=r))
+                        counters=ctx.counters(), rates=r, phases=phases))
     return out
 
 
@@ -440,6 +442,7 @@ def run_mixed(torch, world, dev, stream, s, args, flush, precision, ref_last, re
                                             "duration; the kernel is bound by its FP64 filter, not by the products"}
     else:
         out["dtype"] = "FP32 contraction on the CUDA cores; FP64 filter/weights/sums"
+    out["phase_split"] = rmx[-1]["phases"]
     return out
 
 
@@ -544,6 +547,7 @@ def run_ours(args):
                    "contracted_per_step": last["ncontr"],
                    "work_counters": {"sigma_evals": int(cnt[2]), "window_tests": int(cnt[3]),
                                      "table_builds": int(cnt[4])},
+                   "phase_split": last["phases"],
                    "l2": "256 MiB buffer written between timed steps",
                    "parallelism": f"{world} rank(s), independent solves"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

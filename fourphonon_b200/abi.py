@@ -142,6 +142,13 @@ class Context:
         self._chk(self.lib.fp4_last_counters(self.h, a))
         return list(a)
 
+    def phase_cycles(self):
+        """(work-item cycles, phase-B cycles) of the last four-phonon work kernel,
+        summed over its CTAs (fp4_last_phase_cycles)."""
+        a = (ct.c_int64 * 2)()
+        self._chk(self.lib.fp4_last_phase_cycles(self.h, a))
+        return int(a[0]), int(a[1])
+
     def set_stream(self, stream_handle):
         """Run on an existing cudaStream_t (an int handle, e.g. torch's stream.cuda_stream)."""
         self._chk(self.lib.fp4_set_stream(self.h, ct.c_void_p(stream_handle) if stream_handle else None))

@@ -152,6 +152,13 @@ extern "C" int fp4_last_counters(const fp4_ctx* c, int64_t counters[8]) {
     return FP4_OK;
 }
 
+extern "C" int fp4_last_phase_cycles(const fp4_ctx* c, int64_t cycles[2]) {
+    if (!c || !cycles) return FP4_E_ARG;
+    cycles[0] = c->last_counters[8];
+    cycles[1] = c->last_counters[9];
+    return FP4_OK;
+}
+
 extern "C" int fp4_set_stream(fp4_ctx* c, void* stream) {
     if (!c) return FP4_E_ARG;
     cudaStreamSynchronize(c->stream);
@@ -401,20 +408,20 @@ int fp4_begin(fp4_ctx* c) {
     if (e != cudaSuccess) return fp4_fail(c, FP4_E_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
     int r;
     if ((r = c->b_err.reserve(c, 64))) return r;
-    if ((r = c->b_stats.reserve(c, 64))) return r;
+    if ((r = c->b_stats.reserve(c, 128))) return r;
     c->launches = 0;
     c->kernel_timed = false;
     c->last_tc = false;
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaMemsetAsync(c->b_err.ptr, 0, 64, c->stream));
-    CK(cudaMemsetAsync(c->b_stats.ptr, 0, 64, c->stream));
+    CK(cudaMemsetAsync(c->b_stats.ptr, 0, 128, c->stream));
     return FP4_OK;
 }
 
 int fp4_end(fp4_ctx* c) {
     CK(cudaEventRecord(c->ev1, c->stream));
     int flags = 0;
-    unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long st[16] = {0};
     CK(cudaMemcpyAsync(&flags, c->b_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(st, c->b_stats.ptr, sizeof st, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -430,7 +437,7 @@ int fp4_end(fp4_ctx* c) {
     c->last_launches = c->launches;
     c->last_nproc = (int64_t)st[0];
     c->last_ncontr = (int64_t)st[1];
-    for (int x = 0; x < 8; x++) c->last_counters[x] = (int64_t)st[x];
+    for (int x = 0; x < 16; x++) c->last_counters[x] = (int64_t)st[x];
     c->last_counters[7] = c->last_tc ? 1 : 0;
     if (flags & kErrQueue) return fp4_fail(c, FP4_E_CAPACITY, "an output list or work queue was smaller than the process count");
     if (flags & kErrTable) return fp4_fail(c, FP4_E_CAPACITY, "a device table limit was exceeded");

@@ -60,7 +60,7 @@ struct fp4_ctx {
     IfcTables ifc3, ifc4;
     int64_t last_nproc = 0, last_ncontr = 0, last_launches = 0;
     int last_rta4_nT = 0;  // temperatures of the last four-phonon RTA call (0: none; its partials are in b_part)
-    int64_t last_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t last_counters[16] = {0};  // [0..7] work counters, [8..9] phase cycles
     double last_ms = 0.0, last_kernel_ms = 0.0;
     std::vector<DevBuffer*> all_buffers() {
         std::vector<DevBuffer*> v = {&b_qc, &b_energy, &b_velocity, &b_wv,  &b_eigraw, &b_eig,   &b_eigf,  &b_list,

@@ -771,10 +771,10 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
 }
 
 template <int NT, bool MIXED, bool LIST, bool TC>
-__device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem, const Layout& L,
-                                         const unsigned long long* qbase, const double* qsig, const long long* qpos,
-                                         int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
-                                         unsigned long long& my_contr) {
+__device__ __forceinline__ void k4_flush_body(const P4Params& p, unsigned char* smem, const Layout& L,
+                                              const unsigned long long* qbase, const double* qsig, const long long* qpos,
+                                              int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
+                                              unsigned long long& my_contr) {
     if constexpr (TC) {
         const TcPlan* P = p.tc;
         const Layout Lb = k4_layout_tcbase(NT, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
@@ -787,6 +787,16 @@ __device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem,
     }
 }
 
+template <int NT, bool MIXED, bool LIST, bool TC>
+__device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem, const Layout& L,
+                                         const unsigned long long* qbase, const double* qsig, const long long* qpos,
+                                         int ch, int ii, int q0, int m0, int m1, int m2, int n0, int n1, int n2,
+                                         unsigned long long& my_contr) {
+    const long long t0 = clock64();  // thread 0 adds the CTA's cycles in phase B to stats[9]
+    k4_flush_body<NT, MIXED, LIST, TC>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
+    if (threadIdx.x == 0) atomicAdd(&p.stats[9], (unsigned long long)(clock64() - t0));
+}
+
 // True (for the whole CTA) when some (i,j) queue could overflow within the next
 // kCheckEvery passes of at most one new entry per thread.  The barrier first
 // makes every thread's earlier appends visible: between checks the warps of the
@@ -794,10 +804,12 @@ __device__ __forceinline__ void k4_flush(const P4Params& p, unsigned char* smem,
 // here could be short by that many passes and a queue could overflow.
 __device__ __forceinline__ bool queue_nearly_full(const P4Params& p, const int* cnt, int nb2, int* misc) {
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {  // the largest bin count, over the lanes of warp 0
         int mx = 0;
-        for (int b = 0; b < nb2; b++) mx = max(mx, cnt[b]);
-        misc[2] = (mx > p.subcap - kCheckEvery * (int)blockDim.x);
+        for (int b = threadIdx.x; b < nb2; b += 32) mx = max(mx, cnt[b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (threadIdx.x == 0) misc[2] = (mx > p.subcap - kCheckEvery * (int)blockDim.x);
     }
     __syncthreads();
     return misc[2] != 0;
@@ -1015,6 +1027,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
     unsigned long long& my_contr = st.contr;
     unsigned long long& my_sig = st.sig;
     unsigned long long& my_cand = st.cand;
+    const long long t_item = clock64();  // thread 0 adds the CTA's cycles per work item to stats[8]
     const int ch = wi % 3;
     const int rest = wi / 3;
     const int ii = rest % nptk, ll = rest / nptk;
@@ -1193,6 +1206,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         }
     }
     __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&p.stats[8], (unsigned long long)(clock64() - t_item));
 }
 
 template <int KIND, int NT, bool MIXED>

@@ -395,6 +395,14 @@ int fp4_tc_selftest(int32_t K, int32_t N, const uint16_t *A, const uint16_t *B, 
 int fp4_last_counters(const fp4_ctx *ctx, int64_t counters[8]);
 
 /*
+ * Where the last four-phonon work kernel spent its time, in SM clock cycles
+ * summed over its CTAs: [0] whole work items, [1] the contraction and
+ * weighting of the queued processes (phase B) within them.  [0] - [1] is the
+ * enumeration and energy filter (phase A).  Not part of the reference.
+ */
+int fp4_last_phase_cycles(const fp4_ctx *ctx, int64_t cycles[2]);
+
+/*
  * Run the context's work on an existing CUDA stream (a cudaStream_t passed
  * as void*); NULL restores the context's own stream.  Not part of the
  * reference interface: lets a host that owns a stream order these calls
