@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-sampled", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_simt"], default="fp64",
+                    help="precision of the timed arm (fp64 = the plain drop-in, the benchmarked path)")
     ap.add_argument("--serve-requests", type=int, default=64)
     return ap.parse_args()
 
@@ -463,7 +465,8 @@ def run_ours(args):
         s = workload(cfg, rank)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    ctx = abi.Context(dev, abi.FP4_PREC_FP64)
+    prec = {"fp64": abi.FP4_PREC_FP64, "mixed": abi.FP4_PREC_MIXED, "mixed_simt": abi.FP4_PREC_MIXED_SIMT}
+    ctx = abi.Context(dev, prec[args.precision])
     ctx.set_stream(stream.cuda_stream)
     npi = npi_of(s)
 
@@ -540,8 +543,9 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": cfg["workload"], "config_index": args.config, "grid": [cfg["grid"]] * 3,
+        "dtype": "f64" if args.precision == "fp64" else "f64 filter/weights/sums, " + args.precision + " contraction",
+        "data": "synthetic (seeded)",
+        "config": {"workload": cfg["workload"], "config_index": args.config, "precision": args.precision, "grid": [cfg["grid"]] * 3,
                    "temperatures_K": s.temperatures, "nmodes": s.nmodes, "nbands": s.nb,
                    "ntri4": s.ifc4.ntri, "displacement_classes": npi, "processes_per_step": last["nproc"],
                    "contracted_per_step": last["ncontr"],
