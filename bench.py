@@ -340,8 +340,12 @@ def time_steps(torch, ctx, s, steps, flush):
         e1.record()
         torch.cuda.synchronize()
         nproc, ncontr, call_ms, kms, launches = ctx.stats()
-        item, phb = ctx.phase_cycles()
+        cyc = ctx.phase_cycles(full=True)
+        item, phb = cyc[0], cyc[1]
         phases = {"phase_a_frac": (item - phb) / item if item else None, "phase_b_frac": phb / item if item else None}
+        if cyc[2] or cyc[3]:  # the tensor-core contraction's own split, as fractions of phase B
+            phases.update({"tc_tables_frac_of_b": cyc[2] / phb, "tc_gather_frac_of_b": cyc[3] / phb / 2,
+                           "tc_product_weights_frac_of_b": cyc[4] / phb / 2, "tc_epilogue_frac_of_b": cyc[5] / phb / 2})
         out.append(dict(ms=e0.elapsed_time(e1), kms=kms, nproc=nproc, ncontr=ncontr, launches=launches,
                         counters=ctx.counters(), rates=r, phases=phases))
     return out

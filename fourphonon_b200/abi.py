@@ -142,12 +142,12 @@ class Context:
         self._chk(self.lib.fp4_last_counters(self.h, a))
         return list(a)
 
-    def phase_cycles(self):
+    def phase_cycles(self, full=False):
         """(work-item cycles, phase-B cycles) of the last four-phonon work kernel,
-        summed over its CTAs (fp4_last_phase_cycles)."""
-        a = (ct.c_int64 * 2)()
+        summed over its CTAs; full=True: all eight fields of fp4_last_phase_cycles."""
+        a = (ct.c_int64 * 8)()
         self._chk(self.lib.fp4_last_phase_cycles(self.h, a))
-        return int(a[0]), int(a[1])
+        return [int(x) for x in a] if full else (int(a[0]), int(a[1]))
 
     def set_stream(self, stream_handle):
         """Run on an existing cudaStream_t (an int handle, e.g. torch's stream.cuda_stream)."""

@@ -152,10 +152,9 @@ extern "C" int fp4_last_counters(const fp4_ctx* c, int64_t counters[8]) {
     return FP4_OK;
 }
 
-extern "C" int fp4_last_phase_cycles(const fp4_ctx* c, int64_t cycles[2]) {
+extern "C" int fp4_last_phase_cycles(const fp4_ctx* c, int64_t cycles[8]) {
     if (!c || !cycles) return FP4_E_ARG;
-    cycles[0] = c->last_counters[8];
-    cycles[1] = c->last_counters[9];
+    for (int x = 0; x < 8; x++) cycles[x] = c->last_counters[8 + x];
     return FP4_OK;
 }
 

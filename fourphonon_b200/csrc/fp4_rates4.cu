@@ -595,6 +595,7 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
         __syncthreads();
         const int ng = misc[5], nc = misc[6];
         if (ng == 0 || misc[7]) break;
+        const long long tg0 = clock64();
         // FP64 reciprocal cluster entries of the group's bins
         for (int idx = threadIdx.x; idx < ng * npi * 9; idx += blockDim.x) {
             const int slot = idx / (npi * 9), rem = idx - slot * (npi * 9), pc = rem / 9, sr = rem - pc * 9;
@@ -625,8 +626,10 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
         }
         tc::fence_async_smem();
         __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(&p.stats[10], (unsigned long long)(clock64() - tg0));
         // the chunks: warpgroup wg takes chunks wg, wg+2, ...
         for (int c = wg; c < nc; c += 2) {
+            const long long tc0 = clock64();
             const int code = chunks[c];
             const int slot = code >> 16, e0 = (code & 0xffff) * kTcRows;
             const int bin = gbin[slot], i = bin / nb, j = bin - i * nb;
@@ -648,6 +651,8 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
             tc::fence_async_smem();
             tc::fence_before_sync();
             tc::named_sync(1 + wg, kTcRows);
+            const long long tc1 = clock64();
+            long long tc2 = tc1;
             double wts[NT];
 #pragma unroll
             for (int t = 0; t < NT; t++) wts[t] = 0.0;
@@ -699,6 +704,7 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                 ok = tc::named_all(1 + wg, kTcRows, done);
                 if (!ok) break;  // par stays the parity of the product still pending
                 par ^= 1u;
+                if (pass == 0) tc2 = clock64();
                 tc::fence_after_sync();
                 const float2* e2 = S.eigf + (size_t)(jj * nb + k) * nb;
                 const float2* e3 = S.eigf + (size_t)(ss * nb + l) * nb;
@@ -761,6 +767,12 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                     atomicAdd(&racc[i * NT + t], accr[t]);
                     atomicAdd(&wacc[i * NT + t], accw[t]);
                 }
+            }
+            if (m == 0) {  // cycles of this chunk: gather, product + weights, epilogue
+                const long long tc3 = clock64();
+                atomicAdd(&p.stats[11], (unsigned long long)(tc1 - tc0));
+                atomicAdd(&p.stats[12], (unsigned long long)(tc2 - tc1));
+                atomicAdd(&p.stats[13], (unsigned long long)(tc3 - tc2));
             }
         }
         if (m == 0) slotw[1 + wg] = par;

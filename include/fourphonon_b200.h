@@ -397,10 +397,15 @@ int fp4_last_counters(const fp4_ctx *ctx, int64_t counters[8]);
 /*
  * Where the last four-phonon work kernel spent its time, in SM clock cycles
  * summed over its CTAs: [0] whole work items, [1] the contraction and
- * weighting of the queued processes (phase B) within them.  [0] - [1] is the
- * enumeration and energy filter (phase A).  Not part of the reference.
+ * weighting of the queued processes (phase B) within them ([0] - [1] is the
+ * enumeration and energy filter, phase A).  Tensor-core contraction only,
+ * summed over the CTAs' threads that time them: [2] building the reciprocal
+ * cluster and B tables, and per chunk of 128 processes, summed over the two
+ * warpgroups: [3] gathering the A rows, [4] the product and the weights up
+ * to the end of the wait, [5] the epilogue; [6..7] reserved (0).  Not part of
+ * the reference.
  */
-int fp4_last_phase_cycles(const fp4_ctx *ctx, int64_t cycles[2]);
+int fp4_last_phase_cycles(const fp4_ctx *ctx, int64_t cycles[8]);
 
 /*
  * Run the context's work on an existing CUDA stream (a cudaStream_t passed
