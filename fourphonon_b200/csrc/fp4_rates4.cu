@@ -159,7 +159,7 @@ __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb
 // of one group of bins, two mbarriers, the TMEM address and the parities of the
 // two mbarriers, the group's bins and its chunk list.
 struct TcLayout {
-    size_t a, b, zs, bar, slot, gbin, chunk, total;
+    size_t a, b, zs, eig, plan, bar, slot, gbin, chunk, total;
 };
 
 __host__ __device__ inline Layout k4_layout_tcbase(int NT, int nb, int npi, int ntri, int lsum, int nptk) {
@@ -168,7 +168,7 @@ __host__ __device__ inline Layout k4_layout_tcbase(int NT, int nb, int npi, int 
 }
 
 __host__ __device__ inline TcLayout k4_tc_layout(size_t base, int ksteps, int bin_bytes, int zbins, int npi,
-                                                 int chunk_cap) {
+                                                 int chunk_cap, int nb) {
     TcLayout T;
     size_t o = (base + 127) & ~(size_t)127;
     T.a = o;
@@ -177,6 +177,10 @@ __host__ __device__ inline TcLayout k4_tc_layout(size_t base, int ksteps, int bi
     o += (size_t)zbins * bin_bytes;
     T.zs = o;
     o += (size_t)zbins * npi * 9 * 16;
+    T.eig = o;  // per warpgroup and row: the two eigenvector rows of its process
+    o += (size_t)2 * kTcRows * (2 * nb + 1) * 8;
+    T.plan = o;  // a copy of the plan
+    o = al16(o + sizeof(TcPlan));
     T.bar = o;
     o += 16;
     T.slot = o;
@@ -508,25 +512,34 @@ __device__ void k4_phase_b_all(const P4Params& p, unsigned char* smem, const Lay
 }
 
 // ---------------------------------------------------------------------------- tensor-core phase B
-// One value of a bin's B table: the (n, k) entry of pass `pass`, where n runs over
-// the pass's blocks (32 columns each: re(Z[sr]) at sr, im(Z[sr]) at 9+sr) and k over
-// its classes (6 values each, see TcPlan).  Zero outside the class's own block.
-__device__ __forceinline__ uint16_t tc_b_value(const TcPlan* P, const double2* Zs, int npi, int slot, int pass,
-                                               int n, int k) {
+// 16 bytes (8 bf16 values, k = kb..kb+7) of row n of pass `pass` of a bin's B
+// table: n runs over the pass's blocks (32 columns each: re(Z[sr]) at sr,
+// im(Z[sr]) at 9+sr) and k over its classes (6 values each, see TcPlan); zero
+// outside the class's own block.
+__device__ __forceinline__ uint4 tc_b_chunk(const TcPlan* P, const double2* Zs, int npi, int slot, int pass, int n,
+                                            int kb) {
     const int lb = n >> 5, nn = n & 31;
-    if (nn >= 18) return 0;
     const int4 bk = P->blk[P->pass_blk0[pass] + lb];
-    const int cls = P->pass_cls0[pass] + k / 6;
-    if (cls < bk.x || cls >= bk.y) return 0;
-    const int r6 = k - (k / 6) * 6, split = r6 >> 1, ri = r6 & 1;
-    const int ro = nn >= 9, sr = nn - 9 * ro;
-    const double2 z = Zs[((size_t)slot * npi + cls) * 9 + sr];
-    // the product's real (ro = 0) or imaginary (ro = 1) part takes, from A's
-    // (re, im) pair of w: (Z.re, -Z.im) or (Z.im, Z.re)
-    const double v = (ri == 0) ? (ro == 0 ? z.x : z.y) : (ro == 0 ? -z.y : z.x);
-    uint16_t hi, lo;
-    tc::split_bf16(v, hi, lo);
-    return split == 1 ? lo : hi;
+    const int c0 = P->pass_cls0[pass];
+    const int cls_lo = c0 + kb / 6, cls_hi = c0 + (kb + 7) / 6;
+    uint32_t w4[4] = {0, 0, 0, 0};
+    if (nn < 18 && cls_hi >= bk.x && cls_lo < bk.y) {
+        const int ro = nn >= 9, sr = nn - 9 * ro;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            const int k = kb + y, cls = c0 + k / 6;
+            if (cls < bk.x || cls >= bk.y) continue;
+            const int r6 = k - (k / 6) * 6, split = r6 >> 1, ri = r6 & 1;
+            const double2 z = Zs[((size_t)slot * npi + cls) * 9 + sr];
+            // the product's real (ro = 0) or imaginary (ro = 1) part takes, from A's
+            // (re, im) pair of w: (Z.re, -Z.im) or (Z.im, Z.re)
+            const double v = (ri == 0) ? (ro == 0 ? z.x : z.y) : (ro == 0 ? -z.y : z.x);
+            uint16_t hi, lo;
+            tc::split_bf16(v, hi, lo);
+            w4[y >> 1] |= (uint32_t)(split == 1 ? lo : hi) << (16 * (y & 1));
+        }
+    }
+    return make_uint4(w4[0], w4[1], w4[2], w4[3]);
 }
 
 // Phase B on the tensor cores (mixed precision, RTA): the queued processes of
@@ -538,16 +551,20 @@ __device__ __forceinline__ uint16_t tc_b_value(const TcPlan* P, const double2* Z
 // of the pass, and the epilogue forms V = sum_b u_b^T T_b v_b with u_b the
 // eigenvector of the third phonon on atom a3 of block b (conjugated for the +-
 // and -- channels) and v_b the conjugated eigenvector of the fourth on atom a4.
-// Each warpgroup owns one A tile, one mbarrier and one 128-column TMEM region
-// and takes every other chunk of the group's bins.  The Bose/Gaussian weights
-// are computed in FP64 while the product runs.
+// Each warpgroup owns one A tile, one eigenvector stage, one mbarrier and one
+// 128-column TMEM region and takes every other chunk of the group's bins.  A
+// chunk first issues all its global loads (the phase rows into the A tile, the
+// two eigenvector rows into the stage, the (omega, Bose) records) and forms
+// the FP64 weights; the entry of the warpgroup's next chunk is loaded while
+// the current one runs.  Rate sums stay in registers until the branch i of
+// the chunks changes.
 template <int NT>
 __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layout& L, const TcLayout& TL,
                               const unsigned long long* qbase, const double* qsig, int ch, int ii, int q0,
                               unsigned long long& my_contr) {
     const DevSys& S = p.S;
     const DevIfc& F = p.F;
-    const TcPlan* P = p.tc;
+    const TcPlan* P = reinterpret_cast<const TcPlan*>(smem + TL.plan);
     const int nb = S.nb, nb2 = nb * nb, npi = F.npi;
     const double2* kap = reinterpret_cast<const double2*>(smem + L.kap);
     double* racc = reinterpret_cast<double*>(smem + L.racc);
@@ -569,9 +586,36 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
     const double* wvw = reinterpret_cast<const double*>(S.wv) + 3;
     const uint4* wrows = reinterpret_cast<const uint4*>(p.wtab + (size_t)(ch != 0) * S.nptk * ksteps * 16);
     unsigned char* Aw = Abuf + (size_t)wg * ksteps * kTcRows * 32;
+    // this thread's two eigenvector rows: e''_k then e'''_l (nb components each)
+    // (rows 2*nb+1 float2 apart: an odd stride in 8-byte words keeps the warp's accesses on distinct banks)
+    float2* est = reinterpret_cast<float2*>(smem + TL.eig) + ((size_t)wg * kTcRows + m) * (2 * nb + 1);
     const double sqrtpi = sqrt(3.141592653589793238);
     const double floor_sigma = (double)0.001f;
     constexpr int WS = wb_stride(NT);
+    // the warpgroup's running rate sums of branch cur_i
+    int cur_i = -1;
+    double accr[NT], accw[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        accr[t] = 0.0;
+        accw[t] = 0.0;
+    }
+    auto flush_acc = [&]() {  // warp-uniform: every thread of the warpgroup calls it at the same chunk
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            double r = accr[t], w = accw[t];
+            for (int o = 16; o > 0; o >>= 1) {
+                r += __shfl_down_sync(0xffffffffu, r, o);
+                w += __shfl_down_sync(0xffffffffu, w, o);
+            }
+            if (lane == 0 && t < p.nT && cur_i >= 0) {
+                atomicAdd(&racc[cur_i * NT + t], r);
+                atomicAdd(&wacc[cur_i * NT + t], w);
+            }
+            accr[t] = 0.0;
+            accw[t] = 0.0;
+        }
+    };
     if (threadIdx.x == 0) misc[4] = 0;
     __syncthreads();
     for (;;) {
@@ -615,19 +659,26 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
             const int s = rel / (N * 32), within = rel - s * (N * 32);
             const int n = (within >> 8) * 8 + ((within >> 4) & 7);
             const int kb = s * 16 + ((within >> 7) & 1) * 8;
-            uint32_t w4[4];
-#pragma unroll
-            for (int x = 0; x < 4; x++) {
-                const uint32_t v0 = tc_b_value(P, Zs, npi, slot, pass, n, kb + 2 * x);
-                const uint32_t v1 = tc_b_value(P, Zs, npi, slot, pass, n, kb + 2 * x + 1);
-                w4[x] = v0 | (v1 << 16);
-            }
-            *reinterpret_cast<uint4*>(Bbuf + (size_t)slot * bin_bytes + off) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+            *reinterpret_cast<uint4*>(Bbuf + (size_t)slot * bin_bytes + off) = tc_b_chunk(P, Zs, npi, slot, pass, n, kb);
         }
         tc::fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) atomicAdd(&p.stats[10], (unsigned long long)(clock64() - tg0));
         // the chunks: warpgroup wg takes chunks wg, wg+2, ...
+        unsigned long long ent_n = 0;
+        double sig_n = 0.0;
+        auto load_entry = [&](int c) {
+            if (c < nc) {
+                const int code = chunks[c];
+                const int bin = gbin[code >> 16], e0 = (code & 0xffff) * kTcRows;
+                if (m < min(cnt[bin], p.subcap) - e0) {
+                    const size_t qi = (size_t)bin * p.subcap + e0 + m;
+                    ent_n = qbase[qi];
+                    sig_n = qsig[qi];
+                }
+            }
+        };
+        load_entry(wg);
         for (int c = wg; c < nc; c += 2) {
             const long long tc0 = clock64();
             const int code = chunks[c];
@@ -635,27 +686,74 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
             const int bin = gbin[slot], i = bin / nb, j = bin - i * nb;
             const int n = min(cnt[bin], p.subcap) - e0;
             const bool valid = m < n;
+            const unsigned long long ent = ent_n;
+            double sig = sig_n;
+            load_entry(c + 2);
+            if (i != cur_i) {
+                flush_acc();
+                cur_i = i;
+            }
             int a = 0, b = 0, cc = 0, ss = 0, k = 0, l = 0, jj = 0;
-            double sig = 0.0;
+            double wts[NT];
+#pragma unroll
+            for (int t = 0; t < NT; t++) wts[t] = 0.0;
             if (valid) {
-                const size_t qi = (size_t)bin * p.subcap + e0 + m;
-                unpack_proc(qbase[qi], a, b, cc, ss, k, l);
-                sig = qsig[qi];
+                unpack_proc(ent, a, b, cc, ss, k, l);
                 jj = q_index(S, a, b, cc);
-                // A row m: the phase row of q''
+                // A row m: the phase row of q''; the two eigenvector rows into the stage
                 const uint4* src = wrows + (size_t)jj * ksteps * 2;
-                for (int x = 0; x < 2 * ksteps; x++)
-                    *reinterpret_cast<uint4*>(Aw + (size_t)(x >> 1) * (kTcRows * 32) + tc::kmajor_offset(m, (x & 1) * 8)) =
-                        __ldg(src + x);
+                for (int x0 = 0; x0 < 2 * ksteps; x0 += 2) {  // ksteps*2 words, two loads in flight
+                    uint4 v[2];
+#pragma unroll
+                    for (int y = 0; y < 2; y++)
+                        if (x0 + y < 2 * ksteps) v[y] = __ldg(src + x0 + y);
+#pragma unroll
+                    for (int y = 0; y < 2; y++) {
+                        const int x = x0 + y;
+                        if (x < 2 * ksteps)
+                            *reinterpret_cast<uint4*>(Aw + (size_t)(x >> 1) * (kTcRows * 32) +
+                                                      tc::kmajor_offset(m, (x & 1) * 8)) = v[y];
+                    }
+                }
+                const float2* e2 = S.eigf + (size_t)(jj * nb + k) * nb;
+                const float2* e3 = S.eigf + (size_t)(ss * nb + l) * nb;
+                for (int x = 0; x < nb; x++) {
+                    const float2 u = __ldg(e2 + x), v = __ldg(e3 + x);
+                    est[x] = u;
+                    est[nb + x] = v;
+                }
+                // FP64 weights of every temperature
+                const double* x1 = p.wb + (size_t)(ii * nb + j) * WS;
+                const double* x2 = p.wb + (size_t)(jj * nb + k) * WS;
+                const double* x3 = p.wb + (size_t)(ss * nb + l) * WS;
+                const double omega = wvw[4 * (q0 * nb + i)];
+                const double w1 = x1[0], w2 = x2[0], w3 = x3[0];
+                const double sv = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
+                const double delta =
+                    (ch == 0) ? __dadd_rn(__dadd_rn(sv, w2), -w3) : __dadd_rn(__dadd_rn(sv, -w2), -w3);
+                if (sig <= floor_sigma) sig = 1.0 / sqrtpi;
+                const double g = exp(-(delta * delta) / (sig * sig));
+                const double base = g / (sig * sqrtpi * (omega * w1 * w2 * w3));
+#pragma unroll
+                for (int t = 0; t < NT; t++) {
+                    if (t < p.nT) {
+                        const double f1 = x1[1 + t], f2 = x2[1 + t], f3 = x3[1 + t];
+                        double bc;
+                        if (ch == 0)
+                            bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
+                        else if (ch == 1)
+                            bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
+                        else
+                            bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
+                        wts[t] = bc * base;
+                    }
+                }
             }
             tc::fence_async_smem();
             tc::fence_before_sync();
             tc::named_sync(1 + wg, kTcRows);
             const long long tc1 = clock64();
             long long tc2 = tc1;
-            double wts[NT];
-#pragma unroll
-            for (int t = 0; t < NT; t++) wts[t] = 0.0;
             float2 V = make_float2(0.f, 0.f);
             bool ok = true;
             for (int pass = 0; pass < npass; pass++) {
@@ -672,42 +770,12 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                     tc::commit(tc::smem_u32(&bars[wg]));
                     atomicAdd(&p.stats[6], (unsigned long long)(ksn * (N / 16)));
                 }
-                if (pass == 0 && valid) {
-                    // FP64 weights of every temperature, while the product runs
-                    const double* x1 = p.wb + (size_t)(ii * nb + j) * WS;
-                    const double* x2 = p.wb + (size_t)(jj * nb + k) * WS;
-                    const double* x3 = p.wb + (size_t)(ss * nb + l) * WS;
-                    const double omega = wvw[4 * (q0 * nb + i)];
-                    const double w1 = x1[0], w2 = x2[0], w3 = x3[0];
-                    const double sv = (ch == 2) ? __dadd_rn(omega, -w1) : __dadd_rn(omega, w1);
-                    const double delta =
-                        (ch == 0) ? __dadd_rn(__dadd_rn(sv, w2), -w3) : __dadd_rn(__dadd_rn(sv, -w2), -w3);
-                    if (sig <= floor_sigma) sig = 1.0 / sqrtpi;
-                    const double g = exp(-(delta * delta) / (sig * sig));
-                    const double base = g / (sig * sqrtpi * (omega * w1 * w2 * w3));
-#pragma unroll
-                    for (int t = 0; t < NT; t++) {
-                        if (t < p.nT) {
-                            const double f1 = x1[1 + t], f2 = x2[1 + t], f3 = x3[1 + t];
-                            double bc;
-                            if (ch == 0)
-                                bc = f1 * f2 * (1 + f3) - (1 + f1) * (1 + f2) * f3;
-                            else if (ch == 1)
-                                bc = f1 * (1 + f2) * (1 + f3) - (1 + f1) * f2 * f3;
-                            else
-                                bc = (1 + f1) * (1 + f2) * (1 + f3) - f1 * f2 * f3;
-                            wts[t] = bc * base;
-                        }
-                    }
-                }
                 const bool done = tc::mbar_wait(tc::smem_u32(&bars[wg]), par);
                 ok = tc::named_all(1 + wg, kTcRows, done);
                 if (!ok) break;  // par stays the parity of the product still pending
                 par ^= 1u;
                 if (pass == 0) tc2 = clock64();
                 tc::fence_after_sync();
-                const float2* e2 = S.eigf + (size_t)(jj * nb + k) * nb;
-                const float2* e3 = S.eigf + (size_t)(ss * nb + l) * nb;
                 for (int bl = P->pass_blk0[pass]; bl < P->pass_blk0[pass + 1]; bl++) {
                     const uint32_t col = (uint32_t)((bl - P->pass_blk0[pass]) * 32);
                     float T0[16], T1[16];
@@ -719,9 +787,9 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                         float2 u[3], v[3];
 #pragma unroll
                         for (int x = 0; x < 3; x++) {
-                            u[x] = e2[3 * bk.z + x];
+                            u[x] = est[3 * bk.z + x];
                             if (ch != 0) u[x] = cconjf(u[x]);
-                            v[x] = cconjf(e3[3 * bk.w + x]);
+                            v[x] = cconjf(est[nb + 3 * bk.w + x]);
                         }
                         float2 tt = make_float2(0.f, 0.f);
 #pragma unroll
@@ -749,26 +817,16 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                 }
                 break;
             }
-            double accr[NT], accw[NT];
-            const double v2 = (double)V.x * (double)V.x + (double)V.y * (double)V.y;
+            if (valid) {
+                const double v2 = (double)V.x * (double)V.x + (double)V.y * (double)V.y;
 #pragma unroll
-            for (int t = 0; t < NT; t++) {
-                accr[t] = valid ? wts[t] * v2 : 0.0;
-                accw[t] = valid ? wts[t] : 0.0;
-            }
-            if (valid) my_contr++;
-#pragma unroll
-            for (int t = 0; t < NT; t++) {
-                for (int o = 16; o > 0; o >>= 1) {
-                    accr[t] += __shfl_down_sync(0xffffffffu, accr[t], o);
-                    accw[t] += __shfl_down_sync(0xffffffffu, accw[t], o);
+                for (int t = 0; t < NT; t++) {
+                    accr[t] = fma(wts[t], v2, accr[t]);
+                    accw[t] += wts[t];
                 }
-                if (lane == 0 && t < p.nT) {
-                    atomicAdd(&racc[i * NT + t], accr[t]);
-                    atomicAdd(&wacc[i * NT + t], accw[t]);
-                }
+                my_contr++;
             }
-            if (m == 0) {  // cycles of this chunk: gather, product + weights, epilogue
+            if (m == 0) {  // cycles of this chunk: gather and weights, product, epilogue
                 const long long tc3 = clock64();
                 atomicAdd(&p.stats[11], (unsigned long long)(tc1 - tc0));
                 atomicAdd(&p.stats[12], (unsigned long long)(tc2 - tc1));
@@ -778,6 +836,7 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
         if (m == 0) slotw[1 + wg] = par;
         __syncthreads();
     }
+    flush_acc();
     for (int x = threadIdx.x; x < nb2; x += blockDim.x) cnt[x] = 0;
     __syncthreads();
 }
@@ -790,7 +849,7 @@ __device__ __forceinline__ void k4_flush_body(const P4Params& p, unsigned char* 
     if constexpr (TC) {
         const TcPlan* P = p.tc;
         const Layout Lb = k4_layout_tcbase(NT, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
-        const TcLayout TL = k4_tc_layout(Lb.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap);
+        const TcLayout TL = k4_tc_layout(Lb.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap, p.S.nb);
         k4_phase_b_tc<NT>(p, smem, L, TL, qbase, qsig, ch, ii, q0, my_contr);
     } else if (L.allz) {
         k4_phase_b_all<NT, MIXED, LIST>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2, my_contr);
@@ -1254,11 +1313,16 @@ __global__ void __launch_bounds__(kThreads, 2) k4_work_tc(P4Params p) {
     const int nb2 = p.S.nb * p.S.nb;
     const TcPlan* P = p.tc;
     const Layout L = k4_layout_tcbase(NT, p.S.nb, p.F.npi, p.F.ntri, p.S.n[0] + p.S.n[1] + p.S.n[2], p.S.nptk);
-    const TcLayout TL = k4_tc_layout(L.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap);
+    const TcLayout TL = k4_tc_layout(L.total, P->ksteps, P->bin_bytes, P->zbins, p.F.npi, P->chunk_cap, p.S.nb);
     int* misc = reinterpret_cast<int*>(smem + L.misc);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TL.bar);
     uint32_t* slotw = reinterpret_cast<uint32_t*>(smem + TL.slot);
     k4_cta_init<2, true>(p, smem, L);
+    {  // the plan, copied into shared memory
+        const int* src = reinterpret_cast<const int*>(P);
+        int* dst = reinterpret_cast<int*>(smem + TL.plan);
+        for (int x = threadIdx.x; x < (int)(sizeof(TcPlan) / sizeof(int)); x += blockDim.x) dst[x] = src[x];
+    }
     if (threadIdx.x == 0) {
         tc::mbar_init(tc::smem_u32(&bars[0]), 1);
         tc::mbar_init(tc::smem_u32(&bars[1]), 1);
@@ -1471,7 +1535,7 @@ int k4_tc_plan(int nb, int natoms, int npi, const int* blk_start, int subcap, Tc
 // Shared memory of k4_work_tc for the plan's zbins (the plan's chunk_cap must match).
 size_t k4_tc_smem(int nT, const DevSys& S, const DevIfc& F, const TcPlan& P) {
     const Layout L = k4_layout_tcbase(round_nt(nT), S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], S.nptk);
-    return k4_tc_layout(L.total, P.ksteps, P.bin_bytes, P.zbins, F.npi, P.chunk_cap).total;
+    return k4_tc_layout(L.total, P.ksteps, P.bin_bytes, P.zbins, F.npi, P.chunk_cap, S.nb).total;
 }
 
 int k4_tc_ctas_per_sm() { return 2; }
