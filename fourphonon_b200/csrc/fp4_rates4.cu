@@ -700,27 +700,16 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
             if (valid) {
                 unpack_proc(ent, a, b, cc, ss, k, l);
                 jj = q_index(S, a, b, cc);
-                // A row m: the phase row of q''; the two eigenvector rows into the stage
+                // A row m: the phase row of q''; the two eigenvector rows into the stage.
+                // Asynchronous copies: all in flight at once while the weights are formed.
                 const uint4* src = wrows + (size_t)jj * ksteps * 2;
-                for (int x0 = 0; x0 < 2 * ksteps; x0 += 2) {  // ksteps*2 words, two loads in flight
-                    uint4 v[2];
-#pragma unroll
-                    for (int y = 0; y < 2; y++)
-                        if (x0 + y < 2 * ksteps) v[y] = __ldg(src + x0 + y);
-#pragma unroll
-                    for (int y = 0; y < 2; y++) {
-                        const int x = x0 + y;
-                        if (x < 2 * ksteps)
-                            *reinterpret_cast<uint4*>(Aw + (size_t)(x >> 1) * (kTcRows * 32) +
-                                                      tc::kmajor_offset(m, (x & 1) * 8)) = v[y];
-                    }
-                }
+                for (int x = 0; x < 2 * ksteps; x++)
+                    tc::cp_async16(Aw + (size_t)(x >> 1) * (kTcRows * 32) + tc::kmajor_offset(m, (x & 1) * 8), src + x);
                 const float2* e2 = S.eigf + (size_t)(jj * nb + k) * nb;
                 const float2* e3 = S.eigf + (size_t)(ss * nb + l) * nb;
                 for (int x = 0; x < nb; x++) {
-                    const float2 u = __ldg(e2 + x), v = __ldg(e3 + x);
-                    est[x] = u;
-                    est[nb + x] = v;
+                    tc::cp_async8(est + x, e2 + x);
+                    tc::cp_async8(est + nb + x, e3 + x);
                 }
                 // FP64 weights of every temperature
                 const double* x1 = p.wb + (size_t)(ii * nb + j) * WS;
@@ -748,6 +737,7 @@ __device__ void k4_phase_b_tc(const P4Params& p, unsigned char* smem, const Layo
                         wts[t] = bc * base;
                     }
                 }
+                tc::cp_async_wait_all();
             }
             tc::fence_async_smem();
             tc::fence_before_sync();

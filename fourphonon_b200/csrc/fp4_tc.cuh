@@ -142,6 +142,19 @@ __device__ __forceinline__ bool named_all(int id, int nthreads, bool pred) {
     return r != 0;
 }
 
+// ---------------------------------------------------------------------------- asynchronous copies
+// Global -> shared copies that need no registers (cp.async): 16 bytes (L2 only)
+// or 8 bytes; both addresses aligned to the size.  Wait with cp_async_wait_all().
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------- bf16 splitting
 // x = hi + lo + O(2^-16 |x|): hi = RN_bf16(x), lo = RN_bf16(x - hi).
 __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) {
