@@ -72,10 +72,25 @@ struct CT<true> {
 };
 
 struct Layout {
-    size_t z, kap, pt, sval, swj, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, jjl, misc, total;
+    size_t z, kap, pt, sval, swj, racc, wacc, pacc, red, sidx, cnt, ncnt, klt, pre, blk, seg, jjl, stg, stgi, misc,
+        total;
     int allz;  // 1: the reciprocal cluster tables of all (i,j) at once, 0: one branch i at a time
     int njjl;  // capacity of the list of q'' that the channel's restriction keeps (0: no list)
+    int stgp;  // phase-A passes per stage of (v, omega) records
 };
+
+// Phase A stages the (v, omega) records of the third phonon's grid points of the
+// next stgp passes, and those of the matching fourth-phonon points, in shared
+// memory (at most kStageSlots points per stage), so that a candidate reads them
+// there instead of from global memory.  stgp divides kCheckEvery, so a stage
+// never straddles a queue flush.
+constexpr int kStageSlots = 32;
+__host__ __device__ inline int stage_passes(int nb2) {
+    int P = 8;
+    while (P > 1 && (P * 256 - 1) / nb2 + 2 > kStageSlots) P >>= 1;
+    return P;
+}
+__host__ __device__ inline int stage_slots(int nb2) { return (stage_passes(nb2) * 256 - 1) / nb2 + 2; }
 
 // The +- and -- channels keep a q'' only when q''' >= q''; phase A then walks a list of
 // those q'' (16-bit indices, built per work item) instead of testing every q''.
@@ -132,6 +147,11 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
     o = al16(o + (size_t)(2 * nb + 1) * 8);
     L.jjl = o;
     o = al16(o + (size_t)njjl * 2 + 32 * 4);  // the list, then per-warp counts of the compaction
+    L.stgp = stage_passes((int)nb2);
+    L.stg = o;  // per staged point: the records (v, omega) of its nb branches, then those of its partner
+    o = al16(o + (size_t)stage_slots((int)nb2) * 2 * nb * 32);
+    L.stgi = o;  // per staged point: (its index, its grid coordinates packed, the partner's index)
+    o = al16(o + (size_t)stage_slots((int)nb2) * 16);
     L.misc = o;
     o = al16(o + 8 * 4);
     L.total = o;
@@ -140,17 +160,21 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
 
 // nptk_list: the grid size when the kernel may use the q'' list (0: never).  The list
 // is kept only where it costs no other choice: the all-branch tables come first.
+// The all-branch tables are used while the whole layout keeps the kernel's CTAs
+// per SM resident: kAllZCap for three, kAllZCap2 for two.
+constexpr size_t kAllZCap2 = 110 * 1024;
 __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
                                             int nptk_list) {
     const int nl = (kind == 0 || kind == 2) && nptk_list <= kMaxJJList ? nptk_list : 0;
+    const size_t cap = (kind == 0 || (mixed && NT <= 2)) ? kAllZCap : kAllZCap2;
     if (kind >= 2) {
         Layout A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1, nl);
-        if (A.total <= kAllZCap) return A;
+        if (A.total <= cap) return A;
         A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1, 0);
-        if (A.total <= kAllZCap) return A;
+        if (A.total <= cap) return A;
     }
     Layout B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, nl);
-    if (nl && B.total > kAllZCap) B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, 0);
+    if (nl && B.total > cap) B = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 0, 0);
     return B;
 }
 
@@ -1162,33 +1186,53 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         const int Bq = blockDim.x / nb2, Br = blockDim.x % nb2;
         int cj = threadIdx.x / nb2, ckl = threadIdx.x % nb2;
         int iter = 0;
+        double4* stg = reinterpret_cast<double4*>(smem + L.stg);
+        int4* stgi = reinterpret_cast<int4*>(smem + L.stgi);
+        int stage_first = 0;
         for (int base = 0; base < total; base += blockDim.x, iter++) {
             if (KIND == 2 && (iter % kCheckEvery) == 0) {
                 if (queue_nearly_full(p, cnt, nb2, misc))
                     k4_flush<NT, MIXED, LIST, TC>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                                 my_contr);
             }
+            if ((iter % L.stgp) == 0) {
+                // stage the points of the next stgp passes: their records, their partners and theirs
+                __syncthreads();
+                stage_first = base / nb2;
+                const int nslot = (min(total, base + L.stgp * (int)blockDim.x) - 1) / nb2 - stage_first + 1;
+                for (int x = threadIdx.x; x < nslot * 2 * nb; x += blockDim.x) {
+                    const int slot = x / (2 * nb), r = x - slot * 2 * nb;
+                    const int cjs = stage_first + slot;
+                    const int jj = use_list ? (int)jjl[cjs] : jj_lo + cjs;
+                    int a, b, c;
+                    q_coords_t(S, jj, a, b, c);
+                    int t0, t1, t2;
+                    if (ch == 0) {
+                        t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
+                    } else if (ch == 1) {
+                        t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
+                    } else {
+                        t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
+                    }
+                    const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
+                    stg[x] = (r < nb) ? S.wv[jj * nb + r] : S.wv[ss * nb + (r - nb)];
+                    if (r == 0) stgi[slot] = make_int4(jj, a | (b << 8) | (c << 16), ss, 0);
+                }
+                __syncthreads();
+            }
             if (base + (int)threadIdx.x < total) {
-                const int jj = use_list ? (int)jjl[cj] : jj_lo + cj;
+                const int slot = cj - stage_first;
+                const int4 si = stgi[slot];
+                const int jj = si.x, ss = si.z;
+                const int a = si.y & 0xff, b = (si.y >> 8) & 0xff, c = si.y >> 16;
                 const int kl = klt[ckl];
                 const int k = kl >> 8, l = kl & 0xff;
-                int a, b, c;
-                q_coords_t(S, jj, a, b, c);
-                int t0, t1, t2;
-                if (ch == 0) {
-                    t0 = n0 + m0 + a; t1 = n1 + m1 + b; t2 = n2 + m2 + c;
-                } else if (ch == 1) {
-                    t0 = n0 + m0 - a; t1 = n1 + m1 - b; t2 = n2 + m2 - c;
-                } else {
-                    t0 = n0 - m0 - a; t1 = n1 - m1 - b; t2 = n2 - m2 - c;
-                }
-                const int ss = q_index(S, wrapN(t0, N0), wrapN(t1, N1), wrapN(t2, N2));
                 bool go = true;
                 if (ch != 0 && ss < jj) go = false;
                 if (ch != 0 && ss == jj && l < k) go = false;
                 if (go) {
-                    const double4 w2 = S.wv[jj * nb + k];
-                    const double4 w3 = S.wv[ss * nb + l];
+                    const double4 w2 = stg[slot * 2 * nb + k];
+                    const double4 w3 = stg[slot * 2 * nb + nb + l];
                     if (w2.w != 0.0 && w3.w != 0.0) {
                         const double sigma = sigma_exact(S, w2, w3);
                         my_sig++;
