@@ -230,10 +230,24 @@ __device__ __forceinline__ double div_by_grid(double x, double N, double r) {
     return __fma_rn(e, r, q);
 }
 
+// On a cubic grid all three quotients share N: correct rounding is monotone and
+// symmetric, so RN(RN(dp/N)^2) grows with |dp| and the largest of the three is the
+// one of the largest |dp| -- one division gives the reference's maximum exactly.
 __device__ __forceinline__ double sigma_exact(const DevSys& S, double4 a, double4 b) {
     double v0 = __dadd_rn(a.x, -b.x);
     double v1 = __dadd_rn(a.y, -b.y);
     double v2 = __dadd_rn(a.z, -b.z);
+    if (S.n[0] == S.n[1] && S.n[1] == S.n[2]) {
+        double dmax = 0.0;
+#pragma unroll
+        for (int nu = 0; nu < 3; nu++) {
+            const double* r = S.rl + 3 * nu;
+            const double dp = __dadd_rn(__dadd_rn(__dmul_rn(r[0], v0), __dmul_rn(r[1], v1)), __dmul_rn(r[2], v2));
+            dmax = fmax(dmax, fabs(dp));
+        }
+        const double x = div_by_grid(dmax, S.ngd[0], S.rinv[0]);
+        return __dmul_rn(S.scalebroad, __dsqrt_rn(__dmul_rn(__dmul_rn(x, x), 0.5)));
+    }
     double m = 0.0;
 #pragma unroll
     for (int nu = 0; nu < 3; nu++) {
