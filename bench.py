@@ -70,7 +70,9 @@ def parse():
     ap.add_argument("--no-sampled", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_simt"], default="fp64",
                     help="precision of the timed arm (fp64 = the plain drop-in, the benchmarked path)")
-    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-budget", type=float, default=150.0,
+                    help="estimated serial seconds of the served prefix of the request stream")
+    ap.add_argument("--no-bte", action="store_true")
     return ap.parse_args()
 
 
@@ -528,6 +530,8 @@ def run_ours(args):
 
     if args.config == 3 and not args.no_sampled:
         out["sampled"] = run_sampled(torch, ctx, s, last, flush, 1000.0 * t_max / args.steps)
+    if rank == 0 and world == 1 and not args.no_bte and args.config == 1 and args.precision == "fp64":
+        out["bte"] = run_bte(ctx, s, last["rates"]["rate_4ph"][0], s.temperatures[0])
     if rank == 0 and world == 1 and not args.no_serve and args.config == 1:
         out["serving"] = run_serving(args)
     peak = fp64_dgemm_peak(torch) if rank == 0 else None
@@ -604,81 +608,118 @@ def run_sampled(torch, ctx, s, full, flush, full_ms, nsamples=2_000_000, seed=20
 # ---------------------------------------------------------------------------- serving stream
 
 
+def serial_fp64_solve(ctx, s, T):
+    """One request solved alone through the plain FP64 drivers: 3ph and 4ph RTA
+    rates, tau, iteration0, TConduct and the symmetrised kappa tensor."""
+    r3 = ctx.rta_driver(s, T=T)
+    n = ctx.stats()[0]
+    r4 = ctx.rta_driver_4ph(s, temperatures=[T])
+    n += ctx.stats()[0]
+    rate = r3["rate_plus"] + r3["rate_minus"] + (r4["rate_plusplus"][0] + r4["rate_plusminus"][0]) + \
+        r4["rate_minusminus"][0]
+    tau = np.zeros_like(rate)
+    tau[rate != 0] = 1.0 / rate[rate != 0]
+    F = ctx.iteration0(s, tau)
+    kap = ctx.tconduct(s, F, T=T).reshape(3, 3, s.nb).sum(axis=2).T
+    R = s.sym.crotations
+    return sum(R[r] @ kap @ R[r].T for r in range(len(R))) / len(R), n
+
+
 def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
-    """A Poisson stream of random-cell 3ph+4ph RTA requests through the serving
-    path (mixed precision, continuous batching), against the same cells
-    solved one at a time through the plain FP64 drivers."""
+    """The serving workload: the seeded 512-request stream of random 2-8 atom cells
+    on grids {6,8,10,12,14}^3 at T~U[100,1000] K (system.config4_stream), 3ph+4ph
+    RTA + kappa per request, through the serving path (continuous batching, mixed
+    precision), against the same requests solved one at a time through the plain
+    FP64 drivers.  The whole stream is hours of GPU work (its 8-atom 14^3 requests
+    take minutes each), so a prefix of it is served: the longest one whose
+    estimated serial time fits --serve-budget seconds; the line states it."""
     from fourphonon_b200 import abi, serve
     from fourphonon_b200 import system as S
 
-    pool = S.serving_pool()
-    # serial plain FP64: each pool cell alone, rates + tau + iteration0 + TConduct + symmetrize
+    stream = S.config4_stream(512)
+    rate_est = 2.9e10  # candidate slots per second of the FP64 path (measured order of magnitude)
+    est = [S.request_candidates(na, g) / rate_est for (na, g, T, sd) in stream]
+    full_hours = sum(est) / 3600.0
+    npre, acc = 0, 0.0
+    while npre < len(stream) and (npre < 4 or acc + est[npre] <= args.serve_budget):
+        acc += est[npre]
+        npre += 1
+    specs = stream[:npre]
+    solves = [S.cached_solve(f"random{na}", (g, g, g), (T,), seed=sd) for (na, g, T, sd) in specs]
     ctx = abi.Context(0, abi.FP4_PREC_FP64)
-
-    def serial_solve(s):
-        r3 = ctx.rta_driver(s, T=300.0)
-        n = ctx.stats()[0]
-        r4 = ctx.rta_driver_4ph(s, temperatures=[300.0])
-        n += ctx.stats()[0]
-        rate = r3["rate_plus"] + r3["rate_minus"] + (r4["rate_plusplus"][0] + r4["rate_plusminus"][0]) + \
-            r4["rate_minusminus"][0]
-        tau = np.zeros_like(rate)
-        tau[rate != 0] = 1.0 / rate[rate != 0]
-        F = ctx.iteration0(s, tau)
-        kap = ctx.tconduct(s, F, T=300.0).reshape(3, 3, s.nb).sum(axis=2).T
-        R = s.sym.crotations
-        return sum(R[r] @ kap @ R[r].T for r in range(len(R))) / len(R), n
-
-    # warm-up: every cell once (library load, first allocations of every size), untimed;
-    # then three timed passes, each cell's time the median of its three
-    k64 = [serial_solve(s)[0] for s in pool]
-    passes, nserial = [], 0
-    for _ in range(3):
-        tp = []
-        for s in pool:
-            t0 = time.perf_counter()
-            _, n = serial_solve(s)
-            tp.append(time.perf_counter() - t0)
-            nserial += n
-        passes.append(tp)
+    serial_solve = lambda s, T: serial_fp64_solve(ctx, s, T)  # noqa: E731
+    serial_solve(S.cached_solve("random2", (4, 4, 4), (300.0,), seed=7), 300.0)  # library and allocation warm-up
+    k64, times, nserial = [], [], 0
+    for s, (na, g, T, sd) in zip(solves, specs):
+        t0 = time.perf_counter()
+        k, n = serial_solve(s, T)
+        times.append(time.perf_counter() - t0)
+        k64.append(k)
+        nserial += n
     ctx.close()
-    times = list(np.median(np.array(passes), axis=0))
-    nserial /= 3
     t_serial = float(np.mean(times))
-    rng = np.random.default_rng(20240604)
-    n = max(len(pool), args.serve_requests)
-    rate = 2.0 / t_serial  # arrivals at twice the serial FP64 capacity
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
-    reqs = [serve.Request(float(arrivals[i]), pool[i], 300.0, tag=("pool", i)) for i in range(len(pool))]
-    for i in range(len(pool), n):
-        c = int(rng.integers(len(pool)))
-        reqs.append(serve.Request(float(arrivals[i]), pool[c], float(rng.uniform(100.0, 1000.0)), tag=("rand", c)))
+    rng = np.random.default_rng(20240606)
+    arrivals = np.cumsum(rng.exponential(t_serial / 2.0, size=npre))  # Poisson, twice the serial FP64 rate
+    reqs = [serve.Request(float(arrivals[i]), solves[i], specs[i][2], tag=i) for i in range(npre)]
     precision = abi.FP4_PREC_MIXED if precision is None else precision
-    srv = serve.Server(0, precision, max_slots=max_slots, max_bands=12, hbm_budget=24 << 30)
-    # warm-up: every slot once through (allocates the slots' device buffers), then one
-    # untimed pass of the stream itself
-    warm = [serve.Request(0.0, pool[i % len(pool)], 300.0) for i in range(16)]
+    maxb = max(s.nb for s in solves)
+    srv = serve.Server(0, precision, max_slots=max_slots, max_bands=max(12, maxb), hbm_budget=48 << 30)
+    warm = [serve.Request(0.0, S.cached_solve("random2", (4, 4, 4), (300.0,), seed=7), 300.0)]
     serve.run_stream(srv, warm, tick_items=1 << 16, target_tick_ms=tick_ms)
-    serve.run_stream(srv, [serve.Request(r.arrival, r.solve, r.T) for r in reqs], tick_items=1 << 16,
-                     target_tick_ms=tick_ms)
     done, summ = serve.run_stream(srv, reqs, tick_items=1 << 16, target_tick_ms=tick_ms)
     srv.close()
     kerr = 0.0
     for r in done:
-        if r.tag[0] == "pool":
-            ref = k64[r.tag[1]]
-            if np.abs(ref).max() > 0:
-                kerr = max(kerr, float(np.abs(r.result["kappa"] - ref).max() / np.abs(ref).max()))
-    return {"requests": n, "solves_per_s": summ["solves_per_s"], "p50_ms": summ["p50_ms"], "p99_ms": summ["p99_ms"],
-            "mean_ms": summ["mean_ms"], "processes_per_s": summ["processes_per_s"], "ticks": summ["ticks"],
-            "serial_fp64_solves_per_s": 1.0 / t_serial, "vs_serial_fp64": summ["solves_per_s"] * t_serial,
-            "serial_fp64_processes_per_s": nserial / sum(times),
-            "kappa_rel_err_max": kerr, "precision": "mixed" if precision == abi.FP4_PREC_MIXED else "fp64",
-            "max_slots": max_slots, "tick_ms_target": tick_ms,
-            "host_s": summ["host_s"], "wall_s": summ["wall_s"],
-            "arrivals": "Poisson at twice the serial FP64 rate",
-            "workload": f"{len(pool)} random 2-4 atom cells (masses U[6,120] amu, seeded BvK + Gaussian IFCs), "
-                        "grids 4^3-8^3 with nptk*nbands <= 3072, T~U[100,1000] K, 3ph+4ph RTA + kappa"}
+        ref = k64[r.tag]
+        if np.abs(ref).max() > 0:
+            kerr = max(kerr, float(np.abs(r.result["kappa"] - ref).max() / np.abs(ref).max()))
+    return {"requests": npre, "of_stream": len(stream), "solves_per_s": summ["solves_per_s"],
+            "p50_ms": summ["p50_ms"], "p99_ms": summ["p99_ms"], "mean_ms": summ["mean_ms"],
+            "processes_per_s": summ["processes_per_s"], "ticks": summ["ticks"],
+            "serial_fp64_solves_per_s": npre / sum(times), "vs_serial_fp64": summ["solves_per_s"] * sum(times) / npre,
+            "serial_fp64_processes_per_s": nserial / sum(times), "kappa_rel_err_max": kerr,
+            "precision": "mixed" if precision == abi.FP4_PREC_MIXED else "fp64", "max_slots": max_slots,
+            "tick_ms_target": tick_ms, "host_s": summ["host_s"], "wall_s": summ["wall_s"],
+            "arrivals": "Poisson at twice the serial FP64 rate of the prefix",
+            "prefix": [{"natoms": na, "grid": g, "T": round(T, 1)} for (na, g, T, sd) in specs],
+            "full_stream_estimate_gpu_hours": full_hours,
+            "workload": "seeded stream of 512 random 2-8 atom cells (masses U[6,120] amu, BvK + Gaussian IFCs), "
+                        "grids {6,8,10,12,14}^3, T~U[100,1000] K, 3ph+4ph RTA + kappa; the first `requests` of it"}
+
+
+def run_bte(ctx, s, rate4, T, maxiter=200):
+    """The iterative three-phonon BTE of the benchmarked workload at one temperature:
+    Ind_driver (per-process Gamma and lists), tau from the 3ph+4ph RTA rates,
+    iteration0, then Gauss-Seidel sweeps (iteration, symmetrisation, TConduct)
+    until the relative change of kappa is below 1e-5 (ShengBTE.f90:1271-1306)."""
+    eps = float(np.float32(1e-5))
+    t0 = time.perf_counter()
+    n3 = ctx.np_driver(s)
+    lists = ctx.ind_driver(s, n3[0], n3[1], T=T)
+    ind_ms = ctx.stats()[3]
+    rate = lists["rate_plus"] + lists["rate_minus"] + rate4
+    tau = np.zeros_like(rate)
+    tau[rate != 0] = 1.0 / rate[rate != 0]
+    F = ctx.iteration0(s, tau)
+    k = ctx.tconduct(s, F, T=T).reshape(3, 3, s.nb).sum(axis=2)
+    k_rta = float(np.trace(k) / 3.0)
+    t1 = time.perf_counter()
+    sweep_ms, it = [], 0
+    for it in range(1, maxiter + 1):
+        kold = k
+        F = ctx.iteration(s, F, tau, n3[0], n3[1], lists)
+        sweep_ms.append(ctx.stats()[3])
+        F = ctx.symmetrize_fn(s, F)
+        k = ctx.tconduct(s, F, T=T).reshape(3, 3, s.nb).sum(axis=2)
+        if np.linalg.norm(k - kold) / np.linalg.norm(kold) < eps:
+            break
+    t2 = time.perf_counter()
+    return {"T_K": T, "processes_3ph": int(n3[0].sum() + n3[1].sum()), "ind_driver_kernel_ms": ind_ms,
+            "iterations": it, "sweep_kernel_ms_mean": float(np.mean(sweep_ms)),
+            "sweep_wall_s_mean": (t2 - t1) / it, "to_convergence_wall_s": t2 - t0,
+            "kappa_rta": k_rta, "kappa_converged": float(np.trace(k) / 3.0),
+            "note": "one CTA runs each Gauss-Seidel sweep in the reference's order; wall times include the host "
+                    "calls that pass the process lists"}
 
 
 def main():

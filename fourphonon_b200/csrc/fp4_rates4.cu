@@ -164,9 +164,9 @@ __host__ __device__ inline Layout k4_layout_z(int kind, int NT, bool mixed, int 
 // per SM resident: kAllZCap for three, kAllZCap2 for two.
 constexpr size_t kAllZCap2 = 110 * 1024;
 __host__ __device__ inline Layout k4_layout(int kind, int NT, bool mixed, int nb, int npi, int ntri, int lsum,
-                                            int nptk_list) {
+                                            int nptk_list, size_t cap_override = 0) {
     const int nl = (kind == 0 || kind == 2) && nptk_list <= kMaxJJList ? nptk_list : 0;
-    const size_t cap = (kind == 0 || (mixed && NT <= 2)) ? kAllZCap : kAllZCap2;
+    const size_t cap = cap_override ? cap_override : ((kind == 0 || (mixed && NT <= 2)) ? kAllZCap : kAllZCap2);
     if (kind >= 2) {
         Layout A = k4_layout_z(kind, NT, mixed, nb, npi, ntri, lsum, 1, nl);
         if (A.total <= cap) return A;
@@ -1470,7 +1470,7 @@ __global__ void __launch_bounds__(kThreads, kMultiCtasPerSm) k4_work_multi(const
             int* dst = reinterpret_cast<int*>(&sp);
             for (int x = threadIdx.x; x < (int)(sizeof(P4Params) / sizeof(int)); x += blockDim.x) dst[x] = src[x];
             __syncthreads();
-            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2], 0);
+            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2], 0, kAllZCap);
             k4_cta_init<2, MIXED>(sp, smem, L);
             cur = slot;
         }
@@ -1627,7 +1627,7 @@ cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nbloc
 }
 
 size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F) {
-    return k4_layout(2, 1, mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], 0).total;
+    return k4_layout(2, 1, mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], 0, kAllZCap).total;
 }
 
 cudaError_t prepare_k4_multi(bool mixed, size_t smem) {

@@ -213,6 +213,31 @@ def random_solve(natoms=2, ngrid=(6, 6, 6), temperatures=(300.0,), seed=1, **kw)
     return build_solve(cr, ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, **kw)
 
 
+def config4_stream(n=512, seed=20240604, grids=(6, 8, 10, 12, 14), natoms=(2, 8), temps=(100.0, 1000.0)):
+    """The request stream of the serving workload: n requests, each a random cell of
+    natoms[0]..natoms[1] atoms (crystal.random_cell: masses U[6,120] amu, the seeded
+    BvK + Gaussian cluster generator of the diamond workload), a grid edge drawn from
+    `grids` and T ~ U[temps].  Returns (natoms, grid edge, T, cell seed) per request,
+    in arrival order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        na = int(rng.integers(natoms[0], natoms[1] + 1))
+        g = int(rng.choice(grids))
+        T = float(rng.uniform(*temps))
+        out.append((na, g, T, int(rng.integers(1, 1 << 30))))
+    return out
+
+
+def request_candidates(natoms, grid, nlist=None):
+    """Four-phonon candidate (q', q'', k, l) slots of one RTA solve: 3 channels x
+    nlist x nptk work items of nptk x nbands^2 candidates (nlist ~ nptk/2 for a cell
+    with inversion only when not given)."""
+    nptk = grid ** 3
+    nl = nlist if nlist is not None else nptk // 2 + 4
+    return 3 * nl * nptk * nptk * (3 * natoms) ** 2
+
+
 def serving_pool(n=8, seed=4242, grids=(4, 6, 8), natoms=(2, 3, 4), max_cost=8 ** 3 * 6):
     """n cached random solves for a request stream: cells of natoms atoms on
     grids drawn from `grids`, keeping nptk * nbands <= max_cost so that one
