@@ -518,8 +518,11 @@ static int run_sweep(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int3
             base += t;
         }
     }
+    CK(cudaEventRecord(c->evk0, c->stream));
     k_sweep<<<1, 1024, 0, c->stream>>>(p);
     CK(cudaGetLastError());
+    CK(cudaEventRecord(c->evk1, c->stream));
+    c->kernel_timed = true;
     c->launches++;
     CK(cudaMemcpyAsync(f_n, B[5].ptr, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     B[5].key = 0;  // device copy now differs from the caller's previous F_n

@@ -1470,7 +1470,7 @@ __global__ void __launch_bounds__(kThreads, kMultiCtasPerSm) k4_work_multi(const
             int* dst = reinterpret_cast<int*>(&sp);
             for (int x = threadIdx.x; x < (int)(sizeof(P4Params) / sizeof(int)); x += blockDim.x) dst[x] = src[x];
             __syncthreads();
-            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2], 0, kAllZCap);
+            L = k4_layout(2, NT, MIXED, sp.S.nb, sp.F.npi, sp.F.ntri, sp.S.n[0] + sp.S.n[1] + sp.S.n[2], 0, kAllZCap2);
             k4_cta_init<2, MIXED>(sp, smem, L);
             cur = slot;
         }
@@ -1627,7 +1627,7 @@ cudaError_t launch_k4(int kind, int nT, bool mixed, const P4Params& p, int nbloc
 }
 
 size_t k4_multi_smem(bool mixed, const DevSys& S, const DevIfc& F) {
-    return k4_layout(2, 1, mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], 0, kAllZCap).total;
+    return k4_layout(2, 1, mixed, S.nb, F.npi, F.ntri, S.n[0] + S.n[1] + S.n[2], 0, kAllZCap2).total;
 }
 
 cudaError_t prepare_k4_multi(bool mixed, size_t smem) {

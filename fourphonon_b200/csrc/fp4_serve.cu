@@ -34,7 +34,7 @@ int fp4_setup_ifc(fp4_ctx* c, const fp4_globals* g, int order, int32_t ntri, con
 
 namespace {
 
-constexpr size_t kSmemCap = 72 * 1024;  // dynamic shared memory of the multi-solve kernel
+constexpr size_t kSmemCap = 110 * 1024;  // dynamic shared memory of the multi-solve kernel (2 CTAs per SM)
 
 struct Slot {
     fp4_ctx* ctx = nullptr;

@@ -730,6 +730,29 @@ int64_t fp4o_rta4_strided(const fp4o_sys *s, const fp4o_ifc *f, const int32_t *m
 }
 
 /*
+ * Timing sample of RTA_driver_4ph at the given (mode, q') pairs (0-based), all
+ * three channels each.  Returns the number of surviving processes visited; the
+ * rates are discarded (timing use only).
+ */
+int64_t fp4o_rta4_pairs(const fp4o_sys *s, const fp4o_ifc *f, const int32_t *modes, const int32_t *qps, int n) {
+    int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
+    for (int x = 0; x < n; x++) {
+        const int mm = modes[x] + 1, ii = qps[x];
+        if (!gate(s, mm)) continue;
+        for (int ch = 0; ch < 3; ch++) {
+            acc4_t a;
+            memset(&a, 0, sizeof a);
+            a.ii0 = ii;
+            a.ii1 = ii + 1;
+            proc4_one(s, f, mm, ch, 2, &a);
+            total += a.n;
+        }
+    }
+    return total;
+}
+
+/*
  * Bounded sample of RTA_driver_4ph for timing: modes [mm0,mm1), each
  * restricted to the q' range [ii0,ii1).  Returns the number of surviving
  * processes visited; rates are not normalised (timing use only).

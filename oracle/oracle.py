@@ -46,6 +46,7 @@ def lib():
         _lib.fp4o_num_threads.restype = ct.c_int
         _lib.fp4o_rta4_sample.restype = ct.c_int64
         _lib.fp4o_rta4_strided.restype = ct.c_int64
+        _lib.fp4o_rta4_pairs.restype = ct.c_int64
     return _lib
 
 
@@ -160,6 +161,13 @@ class Oracle:
         m = np.ascontiguousarray(modes, dtype=np.int32)
         return int(lib().fp4o_rta4_strided(ct.byref(self.sys), ct.byref(self.ifc4), _p(m), int(m.size),
                                              int(ii_stride), int(ii_offset)))
+
+    def rta4_pairs(self, modes, qps):
+        """Timing sample: RTA_driver_4ph work at the (mode, q') pairs (0-based);
+        returns the surviving processes visited."""
+        m = np.ascontiguousarray(modes, dtype=np.int32)
+        q = np.ascontiguousarray(qps, dtype=np.int32)
+        return int(lib().fp4o_rta4_pairs(ct.byref(self.sys), ct.byref(self.ifc4), _p(m), _p(q), int(m.size)))
 
     def rta4_sample(self, mm0, mm1, ii0, ii1):
         """Timing sample: RTA_driver_4ph work for modes [mm0,mm1) restricted to
