@@ -408,6 +408,27 @@ class Context:
             _p(F)))
         return F
 
+    def iteration_jacobi(self, s, F, tau_zero, n_plus, n_minus, lists):
+        """One Jacobi sweep (fp4_iteration_jacobi): every step reads F, the new
+        F_n (site symmetrizers applied) is returned."""
+        g = self.globals_of(s)
+        e, v, _, _, _ = self._arrays(s)
+        w = s.wedge
+        nsr = s.sym.nsymm_rot
+        symm = np.ascontiguousarray(np.transpose(s.sym.symmetrizers, (0, 2, 1))).ravel()
+        idq = np.ascontiguousarray(w.id_equi.T, np.int32)
+        n_plus = np.ascontiguousarray(n_plus, np.int32)
+        n_minus = np.ascontiguousarray(n_minus, np.int32)
+        out = np.array(F, dtype=np.float64, copy=True)
+        self._chk(self.lib.fp4_iteration_jacobi(
+            self.h, ct.byref(g), s.nlist, _p(np.ascontiguousarray(w.nequi, np.int32)),
+            _p(np.ascontiguousarray(w.allequi, np.int32)), _p(np.ascontiguousarray(w.typeofsym, np.int32)), nsr,
+            _p(idq), _p(symm), _p(n_plus), _p(n_minus), int(n_plus.sum()), int(n_minus.sum()),
+            _p(lists["ind2_plus"]), _p(lists["ind3_plus"]), _p(lists["ind2_minus"]), _p(lists["ind3_minus"]), _p(e),
+            _p(v), _p(lists["gamma_plus"]), _p(lists["gamma_minus"]), _p(np.ascontiguousarray(tau_zero, np.float64)),
+            _p(out)))
+        return out
+
     def _iteration_4ph(self, s, F, tau_zero, n_plus, n_minus, lists, ind4):
         g = self.globals_of(s)
         e, v, _, _, _ = self._arrays(s)

@@ -58,111 +58,123 @@ __device__ __forceinline__ double& Fat(const BteParams& p, int b, int q, int d) 
     return p.F[((size_t)d * p.nptk + q) * p.nb + b];
 }
 
+// This thread's share (x = t0, t0 + dt, ...) of one step's sum over the mode's
+// processes, with the q-points mapped by symmetry operation `sym`, reading F.
+__device__ __forceinline__ void step_sum(const BteParams& p, const double* F, int mm, int sym, long long t0,
+                                         long long dt, double& a0, double& a1, double& a2) {
+    const int nb = p.nb;
+    auto Fv = [&](int b, int q, int d) { return F[((size_t)d * p.nptk + q) * nb + b]; };
+    const int np_ = p.n_plus[mm], nm_ = p.n_minus[mm];
+    const long long op = p.off_plus[mm], om = p.off_minus[mm];
+    long long c4[3] = {0, 0, 0};
+    if (p.n4[0])
+        for (int ch = 0; ch < 3; ch++) c4[ch] = p.n4[ch][mm];
+    const long long n3ph = (long long)np_ + nm_, ntot = n3ph + c4[0] + c4[1] + c4[2];
+    const long long lim = (long long)p.nptk * nb;
+    for (long long x = t0; x < ntot; x += dt) {
+        if (x >= n3ph) {
+            // iteration_4ph: ++ Gamma(F_l - F_j - F_k), +- Gamma(F_l - F_j + F_k),
+            // -- Gamma(F_l + F_j + F_k), q-points mapped by the same symmetry
+            long long y = x - n3ph;
+            int ch = 0;
+            while (ch < 2 && y >= c4[ch]) {
+                y -= c4[ch];
+                ch++;
+            }
+            const long long o = p.off4[ch][mm] + y;
+            const long long y2 = p.i2_4[ch][o] - 1, y3 = p.i3_4[ch][o] - 1, y4 = p.i4_4[ch][o] - 1;
+            if (y2 < 0 || y2 >= lim || y3 < 0 || y3 >= lim || y4 < 0 || y4 >= lim) {
+                atomicOr(p.err, kErrList);
+                continue;
+            }
+            const int j = (int)(y2 % nb), k = (int)(y3 % nb), l = (int)(y4 % nb);
+            const int qj = p.id_equi[(y2 / nb) * p.nsr + sym] - 1;
+            const int qk = p.id_equi[(y3 / nb) * p.nsr + sym] - 1;
+            const int ql = p.id_equi[(y4 / nb) * p.nsr + sym] - 1;
+            const double g = p.g4[ch][o];
+            const double sj = (ch == 2) ? 1.0 : -1.0, sk = (ch == 0) ? -1.0 : 1.0;
+            // F_l -+ F_j -+ F_k with the reference's left-to-right order
+            a0 += g * ((Fv(l, ql, 0) + sj * Fv(j, qj, 0)) + sk * Fv(k, qk, 0));
+            a1 += g * ((Fv(l, ql, 1) + sj * Fv(j, qj, 1)) + sk * Fv(k, qk, 1));
+            a2 += g * ((Fv(l, ql, 2) + sj * Fv(j, qj, 2)) + sk * Fv(k, qk, 2));
+            continue;
+        }
+        const bool plus = x < np_;
+        const long long o = plus ? op + x : om + (x - np_);
+        const int x2 = (plus ? p.i2p : p.i2m)[o] - 1, x3 = (plus ? p.i3p : p.i3m)[o] - 1;
+        if (x2 < 0 || x2 >= lim || x3 < 0 || x3 >= lim) {
+            atomicOr(p.err, kErrList);
+            continue;
+        }
+        const int j = x2 % nb, m2 = x2 / nb, k = x3 % nb, n3 = x3 / nb;
+        const int qa = p.id_equi[(size_t)n3 * p.nsr + sym] - 1;
+        const int qb = p.id_equi[(size_t)m2 * p.nsr + sym] - 1;
+        const double g = (plus ? p.gp : p.gm)[o];
+        double t0_, t1_, t2_;
+        if (plus) {
+            t0_ = g * (Fv(k, qa, 0) - Fv(j, qb, 0));
+            t1_ = g * (Fv(k, qa, 1) - Fv(j, qb, 1));
+            t2_ = g * (Fv(k, qa, 2) - Fv(j, qb, 2));
+        } else {
+            t0_ = g * (Fv(k, qa, 0) + Fv(j, qb, 0)) * 5.e-1;
+            t1_ = g * (Fv(k, qa, 1) + Fv(j, qb, 1)) * 5.e-1;
+            t2_ = g * (Fv(k, qa, 2) + Fv(j, qb, 2)) * 5.e-1;
+        }
+        a0 += t0_;
+        a1 += t1_;
+        a2 += t2_;
+    }
+}
+
+// Block sum of (a0, a1, a2) into thread 0 (red: 3 x 32 doubles of shared memory).
+__device__ __forceinline__ void block_sum3(double& a0, double& a1, double& a2, double (*red)[32]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_down_sync(0xffffffffu, a0, o);
+        a1 += __shfl_down_sync(0xffffffffu, a1, o);
+        a2 += __shfl_down_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        red[0][warp] = a0;
+        red[1][warp] = a1;
+        red[2][warp] = a2;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        a0 = lane < nwarp ? red[0][lane] : 0.0;
+        a1 = lane < nwarp ? red[1][lane] : 0.0;
+        a2 = lane < nwarp ? red[2][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_down_sync(0xffffffffu, a0, o);
+            a1 += __shfl_down_sync(0xffffffffu, a1, o);
+            a2 += __shfl_down_sync(0xffffffffu, a2, o);
+        }
+    }
+}
+
+// iteration / iteration_4ph (iterations.f90:34-215): one Gauss-Seidel sweep in the
+// reference's order (ll, i, kk), updating F in place; one CTA.
 __global__ void __launch_bounds__(1024) k_sweep(BteParams p) {
     __shared__ double red[3][32];
-    __shared__ double res[3];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int nb = p.nb;
     for (int ll = 0; ll < p.nlist; ll++) {
         for (int i = 0; i < nb; i++) {
             const int mm = ll * nb + i;
-            const int np_ = p.n_plus[mm], nm_ = p.n_minus[mm];
-            const long long op = p.off_plus[mm], om = p.off_minus[mm];
-            long long c4[3] = {0, 0, 0};
-            if (p.n4[0])
-                for (int ch = 0; ch < 3; ch++) c4[ch] = p.n4[ch][mm];
-            const long long n3ph = (long long)np_ + nm_, ntot = n3ph + c4[0] + c4[1] + c4[2];
-            const long long lim = (long long)p.nptk * nb;
             for (int kk = 0; kk < p.nequi[ll]; kk++) {
                 const int qq = p.allequi[ll * p.nsr + kk] - 1;
                 const int sym = p.typeofsym[ll * p.nsr + kk] - 1;
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-                for (long long x = threadIdx.x; x < ntot; x += blockDim.x) {
-                    if (x >= n3ph) {
-                        // iteration_4ph: ++ Gamma(F_l - F_j - F_k), +- Gamma(F_l - F_j + F_k),
-                        // -- Gamma(F_l + F_j + F_k), q-points mapped by the same symmetry
-                        long long y = x - n3ph;
-                        int ch = 0;
-                        while (ch < 2 && y >= c4[ch]) {
-                            y -= c4[ch];
-                            ch++;
-                        }
-                        const long long o = p.off4[ch][mm] + y;
-                        const long long y2 = p.i2_4[ch][o] - 1, y3 = p.i3_4[ch][o] - 1, y4 = p.i4_4[ch][o] - 1;
-                        if (y2 < 0 || y2 >= lim || y3 < 0 || y3 >= lim || y4 < 0 || y4 >= lim) {
-                            atomicOr(p.err, kErrList);
-                            continue;
-                        }
-                        const int j = (int)(y2 % nb), k = (int)(y3 % nb), l = (int)(y4 % nb);
-                        const int qj = p.id_equi[(y2 / nb) * p.nsr + sym] - 1;
-                        const int qk = p.id_equi[(y3 / nb) * p.nsr + sym] - 1;
-                        const int ql = p.id_equi[(y4 / nb) * p.nsr + sym] - 1;
-                        const double g = p.g4[ch][o];
-                        const double sj = (ch == 2) ? 1.0 : -1.0, sk = (ch == 0) ? -1.0 : 1.0;
-                        // F_l -+ F_j -+ F_k with the reference's left-to-right order
-                        a0 += g * ((Fat(p, l, ql, 0) + sj * Fat(p, j, qj, 0)) + sk * Fat(p, k, qk, 0));
-                        a1 += g * ((Fat(p, l, ql, 1) + sj * Fat(p, j, qj, 1)) + sk * Fat(p, k, qk, 1));
-                        a2 += g * ((Fat(p, l, ql, 2) + sj * Fat(p, j, qj, 2)) + sk * Fat(p, k, qk, 2));
-                        continue;
-                    }
-                    const bool plus = x < np_;
-                    const long long o = plus ? op + x : om + (x - np_);
-                    const int x2 = (plus ? p.i2p : p.i2m)[o] - 1, x3 = (plus ? p.i3p : p.i3m)[o] - 1;
-                    if (x2 < 0 || x2 >= lim || x3 < 0 || x3 >= lim) {
-                        atomicOr(p.err, kErrList);
-                        continue;
-                    }
-                    const int j = x2 % nb, m2 = x2 / nb, k = x3 % nb, n3 = x3 / nb;
-                    const int qa = p.id_equi[(size_t)n3 * p.nsr + sym] - 1;
-                    const int qb = p.id_equi[(size_t)m2 * p.nsr + sym] - 1;
-                    const double g = (plus ? p.gp : p.gm)[o];
-                    double t0, t1, t2;
-                    if (plus) {
-                        t0 = g * (Fat(p, k, qa, 0) - Fat(p, j, qb, 0));
-                        t1 = g * (Fat(p, k, qa, 1) - Fat(p, j, qb, 1));
-                        t2 = g * (Fat(p, k, qa, 2) - Fat(p, j, qb, 2));
-                    } else {
-                        t0 = g * (Fat(p, k, qa, 0) + Fat(p, j, qb, 0)) * 5.e-1;
-                        t1 = g * (Fat(p, k, qa, 1) + Fat(p, j, qb, 1)) * 5.e-1;
-                        t2 = g * (Fat(p, k, qa, 2) + Fat(p, j, qb, 2)) * 5.e-1;
-                    }
-                    a0 += t0;
-                    a1 += t1;
-                    a2 += t2;
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    a0 += __shfl_down_sync(0xffffffffu, a0, o);
-                    a1 += __shfl_down_sync(0xffffffffu, a1, o);
-                    a2 += __shfl_down_sync(0xffffffffu, a2, o);
-                }
-                if (lane == 0) {
-                    red[0][warp] = a0;
-                    red[1][warp] = a1;
-                    red[2][warp] = a2;
-                }
-                __syncthreads();
-                if (warp == 0) {
-                    double b0 = lane < nwarp ? red[0][lane] : 0.0;
-                    double b1 = lane < nwarp ? red[1][lane] : 0.0;
-                    double b2 = lane < nwarp ? red[2][lane] : 0.0;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        b0 += __shfl_down_sync(0xffffffffu, b0, o);
-                        b1 += __shfl_down_sync(0xffffffffu, b1, o);
-                        b2 += __shfl_down_sync(0xffffffffu, b2, o);
-                    }
-                    if (lane == 0) {
-                        const double tz = p.tau_zero[ll * nb + i];
-                        const size_t e = (size_t)i * p.nptk + qq, pl = (size_t)p.nptk * nb;
-                        const double w = p.energy[e];
-                        res[0] = tz * p.velocity[e] * w + tz * b0;
-                        res[1] = tz * p.velocity[e + pl] * w + tz * b1;
-                        res[2] = tz * p.velocity[e + 2 * pl] * w + tz * b2;
-                        Fat(p, i, qq, 0) = res[0];
-                        Fat(p, i, qq, 1) = res[1];
-                        Fat(p, i, qq, 2) = res[2];
-                    }
+                step_sum(p, p.F, mm, sym, threadIdx.x, blockDim.x, a0, a1, a2);
+                block_sum3(a0, a1, a2, red);
+                if (threadIdx.x == 0) {
+                    const double tz = p.tau_zero[ll * nb + i];
+                    const size_t e = (size_t)i * p.nptk + qq, pl = (size_t)p.nptk * nb;
+                    const double w = p.energy[e];
+                    Fat(p, i, qq, 0) = tz * p.velocity[e] * w + tz * a0;
+                    Fat(p, i, qq, 1) = tz * p.velocity[e + pl] * w + tz * a1;
+                    Fat(p, i, qq, 2) = tz * p.velocity[e + 2 * pl] * w + tz * a2;
                 }
                 __syncthreads();
                 // F_n(:,qq,:) = transpose(matmul(symmetrizers(:,:,qq), transpose(F_n(:,qq,:))))
@@ -180,6 +192,33 @@ __global__ void __launch_bounds__(1024) k_sweep(BteParams p) {
                 __syncthreads();
             }
         }
+    }
+}
+
+// The Jacobi form of the same update (no counterpart in the reference, whose
+// sweep is Gauss-Seidel): every step reads the previous iterate F and writes
+// Fout, so all steps run at once, one CTA per (mode, equivalent point).  The
+// site symmetrizer is applied afterwards (k_symmetrize) to every point, which is
+// what the in-place sweep's per-step projection does to the band it has just
+// updated.  Converges to the same fixed point, in more sweeps.
+__global__ void __launch_bounds__(256) k_jacobi_step(BteParams p, double* Fout) {
+    __shared__ double red[3][32];
+    const int nb = p.nb;
+    const int mm = blockIdx.x, kk = blockIdx.y;
+    const int ll = mm / nb, i = mm - ll * nb;
+    if (kk >= p.nequi[ll]) return;
+    const int qq = p.allequi[ll * p.nsr + kk] - 1;
+    const int sym = p.typeofsym[ll * p.nsr + kk] - 1;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    step_sum(p, p.F, mm, sym, threadIdx.x, blockDim.x, a0, a1, a2);
+    block_sum3(a0, a1, a2, red);
+    if (threadIdx.x == 0) {
+        const double tz = p.tau_zero[ll * nb + i];
+        const size_t e = (size_t)i * p.nptk + qq, pl = (size_t)p.nptk * nb;
+        const double w = p.energy[e];
+        Fout[((size_t)0 * p.nptk + qq) * nb + i] = tz * p.velocity[e] * w + tz * a0;
+        Fout[((size_t)1 * p.nptk + qq) * nb + i] = tz * p.velocity[e + pl] * w + tz * a1;
+        Fout[((size_t)2 * p.nptk + qq) * nb + i] = tz * p.velocity[e + 2 * pl] * w + tz * a2;
     }
 }
 
@@ -383,7 +422,7 @@ static int run_sweep(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int3
                      const int32_t* n_plus, const int32_t* n_minus, int32_t ntotal_plus, int32_t ntotal_minus,
                      const int32_t* i2p, const int32_t* i3p, const int32_t* i2m, const int32_t* i3m,
                      const double* omega, const double* velocity, const double* gp, const double* gm,
-                     const double* tau_zero, double* f_n, const Lists4* l4) {
+                     const double* tau_zero, double* f_n, const Lists4* l4, bool jacobi = false) {
     if (!c) return FP4_E_ARG;
     int r;
     if ((r = check_g(c, g))) return r;
@@ -518,6 +557,20 @@ static int run_sweep(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int3
             base += t;
         }
     }
+    if (jacobi) {
+        if ((r = B[12].reserve(c, (size_t)nptk * nb * 3 * sizeof(double)))) return r;
+        double* Fout = B[12].as<double>();
+        CK(cudaEventRecord(c->evk0, c->stream));
+        k_jacobi_step<<<dim3((unsigned)nm, (unsigned)nsr), 256, 0, c->stream>>>(p, Fout);
+        CK(cudaGetLastError());
+        k_symmetrize<<<256, 256, 0, c->stream>>>(nb, nptk, B[8].as<double>(), Fout);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->evk1, c->stream));
+        c->kernel_timed = true;
+        c->launches += 2;
+        CK(cudaMemcpyAsync(f_n, Fout, (size_t)nptk * nb * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        return fp4_end(c);
+    }
     CK(cudaEventRecord(c->evk0, c->stream));
     k_sweep<<<1, 1024, 0, c->stream>>>(p);
     CK(cudaGetLastError());
@@ -537,6 +590,17 @@ extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, co
                              const double* gp, const double* gm, const double* tau_zero, double* f_n) {
     return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
                      ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, nullptr);
+}
+
+extern "C" int fp4_iteration_jacobi(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
+                                    const int32_t* allequi, const int32_t* typeofsym, int32_t nsr,
+                                    const int32_t* id_equi, const double* symmetrizers, const int32_t* n_plus,
+                                    const int32_t* n_minus, int32_t ntotal_plus, int32_t ntotal_minus,
+                                    const int32_t* i2p, const int32_t* i3p, const int32_t* i2m, const int32_t* i3m,
+                                    const double* omega, const double* velocity, const double* gp, const double* gm,
+                                    const double* tau_zero, double* f_n) {
+    return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
+                     ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, nullptr, true);
 }
 
 extern "C" int fp4_iteration_4ph(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,

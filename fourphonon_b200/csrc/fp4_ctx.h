@@ -55,7 +55,7 @@ struct fp4_ctx {
     DevBuffer b_queue, b_part, b_work, b_err, b_stats;
     DevBuffer b_tcplan, b_wtab;  // tensor-core contraction: its plan and phase rows
     bool last_tc = false;        // the last four-phonon RTA call ran its contraction on the tensor cores
-    DevBuffer b_bte[12];
+    DevBuffer b_bte[13];  // [12]: the new iterate of a Jacobi sweep
     DevBuffer b_harm[6];  // harmonic stage: pair ranges, terms, images, symmetrizers, outputs, born/masses
     IfcTables ifc3, ifc4;
     int64_t last_nproc = 0, last_ncontr = 0, last_launches = 0;

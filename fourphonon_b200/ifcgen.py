@@ -59,8 +59,11 @@ def _sites_within(cr: Crystal, radius_nm: float, reach: int = 4):
     return out
 
 
-def shell_distances(cr: Crystal, nshell: int = 6):
-    """Sorted distinct interatomic distances (nm) from the basis atoms."""
+def shell_distances(cr: Crystal, nshell: int = 6, rel_tol: float = 0.0):
+    """Sorted distinct interatomic distances (nm) from the basis atoms.  With
+    rel_tol > 0 a distance within rel_tol of the current shell's first one joins
+    that shell (the bonds of a jittered cell), and a shell is represented by its
+    largest member so that every bond of it lies within the shell's radius."""
     sites = _sites_within(cr, 2.0 * np.max(np.linalg.norm(cr.lattvec, axis=0)), reach=3)
     cart = cr.cartesian
     ds = []
@@ -70,6 +73,17 @@ def shell_distances(cr: Crystal, nshell: int = 6):
             if d > 1e-6:
                 ds.append(d)
     ds = np.sort(np.array(ds))
+    if rel_tol > 0.0:
+        shells, first = [ds[0]], ds[0]
+        for d in ds[1:]:
+            if d > first * (1.0 + rel_tol):
+                if len(shells) >= nshell:
+                    break
+                shells.append(d)
+                first = d
+            else:
+                shells[-1] = d
+        return np.array(shells)
     shells = [ds[0]]
     for d in ds[1:]:
         if d - shells[-1] > 1e-4:
@@ -199,24 +213,50 @@ def _canon_set(g):
     return best
 
 
-def bvk_fc2(cr: Crystal, constants, seed_note: str = "") -> dict:
-    """Central-force springs on the first len(constants) neighbour shells.
+def bvk_fc2(cr: Crystal, constants, seed_note: str = "", rel_tol: float = 0.0) -> dict:
+    """Central-force springs on the first len(constants) neighbour shells
+    (shells grouped with shell_distances' rel_tol).
 
     Returns {(a, b, n): 3x3 block} of Phi(a at 0, b at cell n) in eV/A^2.
     """
-    shells = shell_distances(cr, len(constants))
-    rmax = shells[len(constants) - 1] + 1e-4
-    sites = _sites_within(cr, rmax + 0.5, reach=3)
+    shells = shell_distances(cr, len(constants), rel_tol)
     cart = cr.cartesian
+    if rel_tol > 0.0:
+        # per-atom shells: every atom keeps springs to its own nearest neighbours, and a
+        # bond takes the shell that the more distant-neighboured of its two atoms gives it
+        probe = _sites_within(cr, 2.0 * np.max(np.linalg.norm(cr.lattvec, axis=0)), reach=3)
+        own = []
+        for a in range(cr.natoms):
+            ds = np.sort([np.linalg.norm(p - cart[:, a]) for (b, n, p) in probe if np.linalg.norm(p - cart[:, a]) > 1e-6])
+            radii, first = [ds[0]], ds[0]
+            for d in ds[1:]:
+                if d > first * (1.0 + rel_tol):
+                    if len(radii) >= len(constants):
+                        break
+                    radii.append(d)
+                    first = d
+                else:
+                    radii[-1] = d
+            own.append(radii + [radii[-1]] * (len(constants) - len(radii)))
+        own = np.array(own)
+        rmax = float(own.max())
+        shell_of = lambda a, b, r: next((x for x in range(len(constants))  # noqa: E731
+                                         if r <= max(own[a, x], own[b, x]) + 1e-9), None)
+    else:
+        rmax = shells[len(constants) - 1] + 1e-4
+        shell_of = lambda a, b, r: int(np.argmin(np.abs(shells - r))) if r <= rmax else None  # noqa: E731
+    sites = _sites_within(cr, rmax + 0.5, reach=3)
     fc: dict = {}
     for a in range(cr.natoms):
         self_blk = np.zeros((3, 3))
         for (b, n, p) in sites:
             d = p - cart[:, a]
             r = np.linalg.norm(d)
-            if r < 1e-6 or r > rmax:
+            if r < 1e-6 or r > rmax + 1e-9:
                 continue
-            sh = int(np.argmin(np.abs(shells - r)))
+            sh = shell_of(a, b, r)
+            if sh is None:
+                continue
             e = d / r
             k = constants[sh]
             blk = -k * np.outer(e, e)

@@ -120,27 +120,29 @@ def fc2_array(cr: C.Crystal, blocks: dict):
     return H.UNITFACTOR * fc
 
 
-def spring_fc(cr: C.Crystal, seed: int, spring_shells: int = 2, alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6)):
+def spring_fc(cr: C.Crystal, seed: int, spring_shells: int = 2, alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6),
+              shell_tol: float = 0.0):
     """The seeded BvK second-order constants of build_solve: (fc array of
     read2fc, spring constants)."""
     rng = np.random.default_rng(seed)
     consts = [rng.uniform(*alpha_range)]
     for s in range(1, spring_shells):
         consts.append(rng.uniform(*beta_range) * (1.0 if s == 1 else 0.25))
-    return fc2_array(cr, G.bvk_fc2(cr, consts)), consts
+    return fc2_array(cr, G.bvk_fc2(cr, consts, rel_tol=shell_tol)), consts
 
 
 def build_solve(cr: C.Crystal, ngrid, temperatures, seed: int, fc3_shell: int = 3, fc4_shell: int = 1,
                 scalebroad: float = 1.0, with_4ph: bool = True, with_3ph: bool = True, spring_shells: int = 2,
-                alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6)) -> Solve:
+                alpha_range=(2.5, 3.5), beta_range=(0.3, 0.6), shell_tol: float = 0.0) -> Solve:
     """Seeded synthetic solve: BvK springs (alpha per 1NN shell, beta per 2NN
     shell, further shells with beta/4), N(0,5) cubic and N(0,2) quartic
-    clusters within the given neighbour-shell cutoffs."""
-    fc, consts = spring_fc(cr, seed, spring_shells, alpha_range, beta_range)
+    clusters within the given neighbour-shell cutoffs.  shell_tol groups the
+    scattered bond lengths of a jittered cell into shells (relative tolerance)."""
+    fc, consts = spring_fc(cr, seed, spring_shells, alpha_range, beta_range, shell_tol)
     sym = C.build_symmetry(cr, ngrid)
     wd = C.wedge(sym)
     omega, vel, eig = H.eigen_dm(cr, fc, ngrid, sym.symmetrizers)
-    shells = G.shell_distances(cr, max(fc3_shell, fc4_shell) + 1)
+    shells = G.shell_distances(cr, max(fc3_shell, fc4_shell) + 1, shell_tol)
     ifc3 = ifc4 = None
     if with_3ph:
         cut3 = 0.5 * (shells[fc3_shell - 1] + shells[fc3_shell])
@@ -210,7 +212,8 @@ def random_solve(natoms=2, ngrid=(6, 6, 6), temperatures=(300.0,), seed=1, **kw)
     """A random 2-8 atom cell (crystal.random_cell: masses U[6,120] amu) with the
     same seeded BvK + Gaussian cluster generator; the request cells of serving."""
     cr = C.random_cell(np.random.default_rng(seed), natoms)
-    return build_solve(cr, ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, **kw)
+    # the jittered basis scatters the bond lengths: group them into shells within 15 %
+    return build_solve(cr, ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, shell_tol=0.15, **kw)
 
 
 def config4_stream(n=512, seed=20240604, grids=(6, 8, 10, 12, 14), natoms=(2, 8), temps=(100.0, 1000.0)):

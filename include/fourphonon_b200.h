@@ -207,6 +207,23 @@ int fp4_iteration(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32
                   const double *tau_zero, double *f_n);
 
 /*
+ * The Jacobi form of fp4_iteration (no counterpart in the reference, whose
+ * update is Gauss-Seidel, Src/iterations.f90:34-92): same arguments and
+ * layouts; every step of the sweep reads the F_n passed in and the new F_n
+ * (with the site symmetrizers applied) is returned in f_n.  All steps run in
+ * parallel on the device, so a sweep costs milliseconds where the in-order
+ * sweep keeps one CTA busy; the iteration converges to the same kappa in more
+ * sweeps.  Three-phonon processes only.
+ */
+int fp4_iteration_jacobi(fp4_ctx *ctx, const fp4_globals *g, int32_t nlist, const int32_t *nequi,
+                         const int32_t *allequi, const int32_t *typeofsym, int32_t nsymm_rot, const int32_t *id_equi,
+                         const double *symmetrizers, const int32_t *n_plus, const int32_t *n_minus,
+                         int32_t ntotal_plus, int32_t ntotal_minus, const int32_t *ind2_plus, const int32_t *ind3_plus,
+                         const int32_t *ind2_minus, const int32_t *ind3_minus, const double *energy,
+                         const double *velocity, const double *gamma_plus, const double *gamma_minus,
+                         const double *tau_zero, double *f_n);
+
+/*
  * Replaces iteration_4ph (Src/iterations.f90:95-215): the sweep of
  * fp4_iteration with the ++, +- and -- lists of fp4_ind_driver_4ph added
  * (Gamma times F_l-F_j-F_k, F_l-F_j+F_k and F_l+F_j+F_k respectively).
