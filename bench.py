@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--no-sampled", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_simt"], default="fp64",
                     help="precision of the timed arm (fp64 = the plain drop-in, the benchmarked path)")
-    ap.add_argument("--serve-budget", type=float, default=150.0,
+    ap.add_argument("--serve-budget", type=float, default=90.0,
                     help="estimated serial seconds of the served prefix of the request stream")
     ap.add_argument("--no-bte", action="store_true")
     return ap.parse_args()
@@ -498,11 +498,13 @@ def run_ours(args):
     launches = sum(r["launches"] for r in res)
 
     out = {}
+    log(f"fp64: {value:.4g} processes/s, {1000.0 * t_max / args.steps:.0f} ms/step")
     if not args.no_mixed:
         out["mixed"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED, last, value, ctx)
         out["mixed_simt"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED_SIMT, last, value,
                                       ctx)
 
+    log("mixed done" if not args.no_mixed else "mixed skipped")
     # end to end through the public API with host buffers (no upload cache)
     if not args.no_e2e:
         ce = abi.Context(dev, abi.FP4_PREC_FP64)
@@ -528,9 +530,12 @@ def run_ours(args):
     if args.config == 3 and not args.no_sampled:
         out["sampled"] = run_sampled(torch, ctx, s, last, flush, 1000.0 * t_max / args.steps)
     if rank == 0 and world == 1 and not args.no_bte and args.config == 1 and args.precision == "fp64":
+        log("bte ...")
         out["bte"] = run_bte(ctx, s, last["rates"]["rate_4ph"][0], s.temperatures[0])
     if rank == 0 and world == 1 and not args.no_serve and args.config == 1:
+        log("serving ...")
         out["serving"] = run_serving(args)
+        log("serving done")
     peak = fp64_dgemm_peak(torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -634,13 +639,13 @@ def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
     from fourphonon_b200 import system as S
 
     stream = S.config4_stream(512)
-    rate_est = 2.9e10  # candidate slots per second of the FP64 path (measured order of magnitude)
-    est = [S.request_candidates(na, g) / rate_est for (na, g, T, sd) in stream]
+    est = [S.request_seconds(na, g) for (na, g, T, sd) in stream]
     full_hours = sum(est) / 3600.0
     npre, acc = 0, 0.0
-    while npre < len(stream) and (npre < 4 or acc + est[npre] <= args.serve_budget):
+    while npre < len(stream) and acc + est[npre] <= args.serve_budget:
         acc += est[npre]
         npre += 1
+    npre = max(npre, 1)
     specs = stream[:npre]
     solves = [S.cached_solve(f"random{na}", (g, g, g), (T,), seed=sd) for (na, g, T, sd) in specs]
     ctx = abi.Context(0, abi.FP4_PREC_FP64)
@@ -679,7 +684,7 @@ def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
             "tick_ms_target": tick_ms, "host_s": summ["host_s"], "wall_s": summ["wall_s"],
             "arrivals": "Poisson at twice the serial FP64 rate of the prefix",
             "prefix": [{"natoms": na, "grid": g, "T": round(T, 1)} for (na, g, T, sd) in specs],
-            "full_stream_estimate_gpu_hours": full_hours,
+            "full_stream_estimate_gpu_hours": full_hours, "prefix_estimate_serial_s": acc,
             "workload": "seeded stream of 512 random 2-8 atom cells (masses U[6,120] amu, BvK + Gaussian IFCs), "
                         "grids {6,8,10,12,14}^3, T~U[100,1000] K, 3ph+4ph RTA + kappa; the first `requests` of it"}
 

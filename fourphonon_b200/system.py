@@ -241,6 +241,18 @@ def request_candidates(natoms, grid, nlist=None):
     return 3 * nl * nptk * nptk * (3 * natoms) ** 2
 
 
+def request_seconds(natoms, grid, nlist=None):
+    """Rough plain-FP64 time of one four-phonon RTA solve on one B200: the filter
+    per candidate slot plus the contraction per surviving process, whose number
+    grows as nbands^4 (the windows of the nbands^2 sorted pair sums fill up).
+    Constants from the 16^3 diamond workload (1.6e-11 s per slot, 2.2 % of
+    nptk^2 nlist nbands^4 survive, 9e-11 s per survivor)."""
+    nptk = grid ** 3
+    nl = nlist if nlist is not None else nptk // 2 + 4
+    nb = 3 * natoms
+    return 1.6e-11 * request_candidates(natoms, grid, nl) + 9e-11 * 0.0217 * nptk * nptk * nl * nb ** 4
+
+
 def serving_pool(n=8, seed=4242, grids=(4, 6, 8), natoms=(2, 3, 4), max_cost=8 ** 3 * 6):
     """n cached random solves for a request stream: cells of natoms atoms on
     grids drawn from `grids`, keeping nptk * nbands <= max_cost so that one

@@ -3,7 +3,7 @@ reference's Gauss-Seidel sweep (fp4_iteration, iterations.f90:34-92).
 
 Both iterate the same linear map, so they share its fixed point: the F_n that
 the Jacobi sweeps converge to is left unchanged by one in-order sweep (within
-1e-9), and the converged kappa of the two agree (within 1e-6).  A Jacobi sweep
+1e-8), and the converged kappa of the two agree (within 1e-6).  A Jacobi sweep
 is also deterministic (fixed summation order).
 """
 import numpy as np
@@ -57,7 +57,7 @@ def test_jacobi_and_gauss_seidel_share_the_fixed_point():
         Fs = ctx.iteration(s, Fj.copy(), tau, n_p, n_m, lists)
         Fs = ctx.symmetrize_fn(s, Fs)
         scale = np.abs(Fj).max()
-        assert np.abs(Fs - Fj).max() <= 1e-9 * scale
+        assert np.abs(Fs - Fj).max() <= 1e-8 * scale
         # a sweep's sums run in a fixed order: the same input gives the same output, bit for bit
         a = ctx.iteration_jacobi(s, F0.copy(), tau, n_p, n_m, lists)
         b = ctx.iteration_jacobi(s, F0.copy(), tau, n_p, n_m, lists)
