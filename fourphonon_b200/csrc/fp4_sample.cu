@@ -113,12 +113,66 @@ __device__ double2 vp4_direct(const DevSys& S, const DevIfc& F, int ch, const do
     return V;
 }
 
+// The same sum in FP32 (mixed precision): FP32 eigenvectors and root tables,
+// the cluster constants rounded to FP32 as they are read, FP32 accumulation.
+__device__ float2 vp4_direct_f(const DevSys& S, const DevIfc& F, int ch, const float2* ei, const float2* ej,
+                               const float2* ek, const float2* el, int m0, int m1, int m2, int a0, int a1, int a2,
+                               int t0, int t1, int t2) {
+    const int sj = (ch == 2) ? -1 : 1, sk = (ch == 0) ? 1 : -1;
+    float2 V = make_float2(0.f, 0.f);
+    for (int c = 0; c < F.ntri; c++) {
+        const int4 at = F.atoms[c];
+        const int4 mj = F.mj[c], mk = F.mk[c], ml = F.ml[c];
+        const float2 ph =
+            cmulf(cmulf(S.rootf[0][pmod(sj * m0 * mj.x + sk * a0 * mk.x - t0 * ml.x, S.n[0])],
+                        S.rootf[1][pmod(sj * m1 * mj.y + sk * a1 * mk.y - t1 * ml.y, S.n[1])]),
+                  S.rootf[2][pmod(sj * m2 * mj.z + sk * a2 * mk.z - t2 * ml.z, S.n[2])]);
+        float2 I[3], J[3], K[3], L[3];
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            I[x] = ei[3 * at.x + x];
+            J[x] = ej[3 * at.y + x];
+            if (ch == 2) J[x] = cconjf(J[x]);
+            K[x] = ek[3 * at.z + x];
+            if (ch != 0) K[x] = cconjf(K[x]);
+            L[x] = cconjf(el[3 * at.w + x]);
+        }
+        const double* psi = F.phi + (size_t)c * 81;
+        float2 A = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            float2 wu = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int t = 0; t < 3; t++) {
+                float2 y = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int s = 0; s < 3; s++) {
+                    const double* row = psi + ((u * 3 + t) * 3 + s) * 3;
+                    float2 xs = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        const float f = (float)row[r];
+                        xs.x = fmaf(f, L[r].x, xs.x);
+                        xs.y = fmaf(f, L[r].y, xs.y);
+                    }
+                    y = cmacf(y, xs, K[s]);
+                }
+                wu = cmacf(wu, y, J[t]);
+            }
+            A = cmacf(A, wu, I[u]);
+        }
+        const float mu = (float)F.mu[c];
+        V = cmacf(V, make_float2(mu * ph.x, mu * ph.y), A);
+    }
+    return V;
+}
+
 struct SEntry {
     int ii, jj, ss, jkl;
     double sigma, delta;
 };
 
-template <int NT>
+template <int NT, bool MIXED>
 __global__ void __launch_bounds__(kSThreads) k4_sample(PSParams p) {
     __shared__ SEntry q[kSChunk];
     __shared__ int s_cnt, s_item;
@@ -221,11 +275,20 @@ __global__ void __launch_bounds__(kSThreads) k4_sample(PSParams p) {
                     q_coords_t(S, en.ii, m0c, m1c, m2c);
                     q_coords_t(S, en.jj, a, b, cc);
                     q_coords_t(S, en.ss, t0, t1, t2);
-                    const double2 V = vp4_direct(S, p.F, ch, ei, S.eig + (size_t)(en.ii * nb + j) * nb,
-                                                 S.eig + (size_t)(en.jj * nb + k) * nb,
-                                                 S.eig + (size_t)(en.ss * nb + l) * nb, m0c, m1c, m2c, a, b, cc, t0,
-                                                 t1, t2);
-                    v2 = V.x * V.x + V.y * V.y;
+                    if (MIXED) {
+                        const float2* eif = S.eigf + (size_t)(q0 * nb + i) * nb;
+                        const float2 V = vp4_direct_f(S, p.F, ch, eif, S.eigf + (size_t)(en.ii * nb + j) * nb,
+                                                      S.eigf + (size_t)(en.jj * nb + k) * nb,
+                                                      S.eigf + (size_t)(en.ss * nb + l) * nb, m0c, m1c, m2c, a, b,
+                                                      cc, t0, t1, t2);
+                        v2 = (double)V.x * (double)V.x + (double)V.y * (double)V.y;
+                    } else {
+                        const double2 V = vp4_direct(S, p.F, ch, ei, S.eig + (size_t)(en.ii * nb + j) * nb,
+                                                     S.eig + (size_t)(en.jj * nb + k) * nb,
+                                                     S.eig + (size_t)(en.ss * nb + l) * nb, m0c, m1c, m2c, a, b, cc,
+                                                     t0, t1, t2);
+                        v2 = V.x * V.x + V.y * V.y;
+                    }
                 }
                 const double g = exp(-(en.delta * en.delta) / (en.sigma * en.sigma));
                 const bool low = (w1 <= 1.25 || w2 <= 1.25 || w3 <= 1.25);
@@ -525,14 +588,23 @@ static int run_sample(fp4_ctx* c, int mode, int nT, const double* temps, int64_t
     p.err = c->b_err.as<int>();
     const int nblocks = (int)std::min<int64_t>(nitems, (int64_t)c->sm_count * 8);
     CK(cudaEventRecord(c->evk0, c->stream));
-    if (mode == 2 && nt > 4)
-        k4_sample<8><<<nblocks, kSThreads, 0, c->stream>>>(p);
-    else if (mode == 2 && nt > 2)
-        k4_sample<4><<<nblocks, kSThreads, 0, c->stream>>>(p);
-    else if (mode == 2 && nt > 1)
-        k4_sample<2><<<nblocks, kSThreads, 0, c->stream>>>(p);
-    else
-        k4_sample<1><<<nblocks, kSThreads, 0, c->stream>>>(p);
+    // mixed precision: the V(4) sums in FP32 (the draws, filter, weights and sums stay FP64)
+    const bool mixed = mode == 2 && c->precision != FP4_PREC_FP64;
+#define FP4_KS(NTV)                                                   \
+    if (mixed)                                                        \
+        k4_sample<NTV, true><<<nblocks, kSThreads, 0, c->stream>>>(p); \
+    else                                                              \
+        k4_sample<NTV, false><<<nblocks, kSThreads, 0, c->stream>>>(p);
+    if (mode == 2 && nt > 4) {
+        FP4_KS(8)
+    } else if (mode == 2 && nt > 2) {
+        FP4_KS(4)
+    } else if (mode == 2 && nt > 1) {
+        FP4_KS(2)
+    } else {
+        FP4_KS(1)
+    }
+#undef FP4_KS
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->evk1, c->stream));
     c->kernel_timed = true;
