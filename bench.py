@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-sampled", action="store_true")
+    ap.add_argument("--mixed-modes", default="mixed,mixed_simt",
+                    help="mixed precisions timed beside FP64: mixed (tensor cores), mixed_simt (CUDA cores)")
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_simt"], default="fp64",
                     help="precision of the timed arm (fp64 = the plain drop-in, the benchmarked path)")
     ap.add_argument("--serve-budget", type=float, default=90.0,
@@ -500,9 +502,12 @@ def run_ours(args):
     out = {}
     log(f"fp64: {value:.4g} processes/s, {1000.0 * t_max / args.steps:.0f} ms/step")
     if not args.no_mixed:
-        out["mixed"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED, last, value, ctx)
-        out["mixed_simt"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED_SIMT, last, value,
-                                      ctx)
+        modes = args.mixed_modes.split(",")
+        if "mixed" in modes:
+            out["mixed"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED, last, value, ctx)
+        if "mixed_simt" in modes:
+            out["mixed_simt"] = run_mixed(torch, world, dev, stream, s, args, flush, abi.FP4_PREC_MIXED_SIMT, last,
+                                          value, ctx)
 
     log("mixed done" if not args.no_mixed else "mixed skipped")
     # end to end through the public API with host buffers (no upload cache)
@@ -585,26 +590,46 @@ def run_ours(args):
 
 
 def run_sampled(torch, ctx, s, full, flush, full_ms, nsamples=2_000_000, seed=20240605):
-    """The sampled estimator of the same workload (FP64): its time and the error
-    of its rates against the full enumeration, summed over modes and per mode."""
-    flush.zero_()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    r = ctx.rta_driver_4ph_sample(s, nsamples, seed)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    errs = {}
-    for t, T in enumerate(s.temperatures):
-        f = full["rates"]["rate_4ph"][t]
-        g = r["rate_plusplus"][t] + r["rate_plusminus"][t] + r["rate_minusminus"][t]
-        m = f > 1e-6 * f.max()
-        rel = np.abs(g[m] - f[m]) / f[m]
-        errs[f"{T:.0f}K"] = {"sum_rel_err": float(abs(g.sum() - f.sum()) / f.sum()),
-                             "per_mode_median": float(np.median(rel)), "per_mode_p90": float(np.percentile(rel, 90))}
-    return {"nsamples_per_mode_channel": nsamples, "ms": ms, "speedup_vs_full": full_ms / ms,
-            "errors_vs_full": errs, "dtype": "f64"}
+    """The sampled estimator of the same workload, in FP64 and in mixed precision
+    (FP32 V(4) sums): its time and the error of its rates against the full FP64
+    enumeration, summed over modes and per mode; and mixed against FP64 on the
+    same draws."""
+    from fourphonon_b200 import abi
+
+    out = {"nsamples_per_mode_channel": nsamples}
+    rates = {}
+    for name, prec in (("fp64", abi.FP4_PREC_FP64), ("mixed", abi.FP4_PREC_MIXED)):
+        c = abi.Context(torch.cuda.current_device(), prec)
+        c.set_stream(torch.cuda.current_stream().cuda_stream)
+        c.rta_driver_4ph_sample(s, 1000, seed)  # allocations
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = c.rta_driver_4ph_sample(s, nsamples, seed)
+        e1.record()
+        torch.cuda.synchronize()
+        c.close()
+        ms = e0.elapsed_time(e1)
+        errs = {}
+        for t, T in enumerate(s.temperatures):
+            f = full["rates"]["rate_4ph"][t]
+            g = r["rate_plusplus"][t] + r["rate_plusminus"][t] + r["rate_minusminus"][t]
+            m = f > 1e-6 * f.max()
+            rel = np.abs(g[m] - f[m]) / f[m]
+            errs[f"{T:.0f}K"] = {"sum_rel_err": float(abs(g.sum() - f.sum()) / f.sum()),
+                                 "per_mode_median": float(np.median(rel)),
+                                 "per_mode_p90": float(np.percentile(rel, 90))}
+        rates[name] = r
+        out[name] = {"ms": ms, "speedup_vs_full_fp64": full_ms / ms, "errors_vs_full_fp64": errs}
+    worst = 0.0
+    for t in range(len(s.temperatures)):
+        a = sum(rates["fp64"]["rate_" + ch][t] for ch in ("plusplus", "plusminus", "minusminus"))
+        b = sum(rates["mixed"]["rate_" + ch][t] for ch in ("plusplus", "plusminus", "minusminus"))
+        m = a > 1e-6 * a.max()
+        worst = max(worst, float(np.max(np.abs(b[m] - a[m]) / a[m])))
+    out["mixed"]["rate_rel_err_vs_fp64_same_draws"] = worst
+    return out
 
 
 # ---------------------------------------------------------------------------- serving stream
