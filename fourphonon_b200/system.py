@@ -212,7 +212,9 @@ def random_solve(natoms=2, ngrid=(6, 6, 6), temperatures=(300.0,), seed=1, **kw)
     """A random 2-8 atom cell (crystal.random_cell: masses U[6,120] amu) with the
     same seeded BvK + Gaussian cluster generator; the request cells of serving."""
     cr = C.random_cell(np.random.default_rng(seed), natoms)
-    # the jittered basis scatters the bond lengths: group them into shells within 15 %
+    # the jittered basis scatters the bond lengths: group them into shells within 15 %, and
+    # spring three shells per atom (two leave some 7-8 atom cells with zero-energy mechanisms)
+    kw.setdefault("spring_shells", 3)
     return build_solve(cr, ngrid, temperatures, seed, fc3_shell=3, fc4_shell=1, shell_tol=0.15, **kw)
 
 
