@@ -208,6 +208,16 @@ __device__ __forceinline__ int lower_bound_desc(const double* a, int n, double x
     }
     return i;
 }
+// First index i with a[i] > x (the count of entries <= x), by the same descent.
+__device__ __forceinline__ int upper_bound_desc(const double* a, int n, double x) {
+    int i = 0;
+    if (n <= 0) return 0;
+    for (int step = 1 << (31 - __clz(n)); step > 0; step >>= 1) {
+        const int y = i + step;
+        if (y <= n && a[y - 1] <= x) i = y;
+    }
+    return i;
+}
 
 // ---------------------------------------------------------------------------
 // Energy-conservation filter, bit-exact with the reference's source order.

@@ -1220,11 +1220,16 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                 }
                 __syncthreads();
             }
+            // This lane's candidate (q'', k, l): sigma, and the window [lo, lo + n) of the
+            // sorted sums that can pass the 1-sigma test.
+            int n = 0, lo = 0, jj = 0;
+            double w2w = 0.0, w3w = 0.0, sigma = 0.0;
+            unsigned long long pk = 0;
             if (base + (int)threadIdx.x < total) {
                 const int slot = cj - stage_first;
                 const int4 si = stgi[slot];
-                const int jj = si.x, ss = si.z;
-                const int a = si.y & 0xff, b = (si.y >> 8) & 0xff, c = si.y >> 16;
+                jj = si.x;
+                const int ss = si.z;
                 const int kl = klt[ckl];
                 const int k = kl >> 8, l = kl & 0xff;
                 bool go = true;
@@ -1234,47 +1239,78 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                     const double4 w2 = stg[slot * 2 * nb + k];
                     const double4 w3 = stg[slot * 2 * nb + nb + l];
                     if (w2.w != 0.0 && w3.w != 0.0) {
-                        const double sigma = sigma_exact(S, w2, w3);
+                        sigma = sigma_exact(S, w2, w3);
                         my_sig++;
                         const double cen = (ch == 0) ? (w3.w - w2.w) : (w2.w + w3.w);
                         const double tol = 1e-12 * (1.0 + fabs(w2.w) + fabs(w3.w) + smax + sigma);
-                        int x = lower_bound_desc(sval, ns, cen - sigma - tol);
-                        for (; x < ns && sval[x] <= cen + sigma + tol; x++) {
-                            my_cand++;
-                            const double s = sval[x];
-                            const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, w2.w), -w3.w)
-                                                           : __dadd_rn(__dadd_rn(s, -w2.w), -w3.w);
-                            if (!(fabs(delta) <= sigma)) continue;
-                            const int ij = sidx[x];
-                            const int i = ij >> 16, j = ij & 0xffff;
-                            const int idx = i * nb + j;
-                            if (ch != 1 && jj == ii && k < j) continue;
-                            if (ch == 1 && !((q0 != jj || i != k) && (q0 != ss || i != l) && (ii != jj || j != k) &&
-                                             (ii != ss || j != l)))
-                                continue;
-                            my_surv++;
-                            if (KIND == 0) {
-                                const double sg = (sigma <= floor_sigma) ? 1.0 / sqrtpi : sigma;
-                                const double pc = exp(-(delta * delta) / (sg * sg)) /
-                                                  (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
-                                                   (double)(nb * nb * nb * nb));
-                                const int o = (threadIdx.x >> 5) * nb + i;
-                                atomicAdd(&ncnt[o], 1);
-                                atomicAdd(&pacc[o], pc);
-                                continue;
-                            }
-                            const double w1 = swj[x];
-                            if (w1 <= 1.25 || w2.w <= 1.25 || w3.w <= 1.25) continue;  // WP4 = 0 exactly
-                            const int pos = atomicAdd(&cnt[idx], 1);
-                            if (pos >= p.subcap) {  // cannot happen with the capacity checks
-                                atomicOr(p.err, kErrQueue);
-                                continue;
-                            }
-                            qbase[(size_t)idx * p.subcap + pos] = pack_proc(a, b, c, ss, k, l);
-                            qsig[(size_t)idx * p.subcap + pos] = sigma;
-                        }
+                        lo = lower_bound_desc(sval, ns, cen - sigma - tol);
+                        n = max(0, upper_bound_desc(sval, ns, cen + sigma + tol) - lo);
+                        w2w = w2.w;
+                        w3w = w3.w;
+                        pk = pack_proc(si.y & 0xff, (si.y >> 8) & 0xff, si.y >> 16, ss, k, l);
                     }
                 }
+            }
+            // The windows differ in length from lane to lane.  Their entries are dealt
+            // out over the warp's lanes (an inclusive scan of the lengths; entry e
+            // belongs to the first lane whose prefix exceeds e), so the exact test and
+            // the queue append run with every lane busy instead of for as many
+            // iterations as the longest window.
+            const int lane = threadIdx.x & 31;
+            int incl = n;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+            for (int r0 = 0; r0 < wtot; r0 += 32) {
+                const int e = r0 + lane;
+                int src = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (__shfl_sync(0xffffffffu, incl, src + step - 1) <= e) src += step;
+                const int x = __shfl_sync(0xffffffffu, lo - (incl - n), src) + e;
+                const double ew2 = __shfl_sync(0xffffffffu, w2w, src);
+                const double ew3 = __shfl_sync(0xffffffffu, w3w, src);
+                const double esg = __shfl_sync(0xffffffffu, sigma, src);
+                const unsigned long long epk = __shfl_sync(0xffffffffu, pk, src);
+                const int ejj = __shfl_sync(0xffffffffu, jj, src);
+                if (e >= wtot) continue;
+                my_cand++;
+                const double s = sval[x];
+                const double delta = (ch == 0) ? __dadd_rn(__dadd_rn(s, ew2), -ew3)
+                                               : __dadd_rn(__dadd_rn(s, -ew2), -ew3);
+                if (!(fabs(delta) <= esg)) continue;
+                const int ij = sidx[x];
+                const int i = ij >> 16, j = ij & 0xffff;
+                const int idx = i * nb + j;
+                const int k = (int)((epk >> 8) & 0xff), l = (int)(epk & 0xff);
+                const int ss = (int)((epk >> 16) & 0x3ffff);
+                if (ch != 1 && ejj == ii && k < j) continue;
+                if (ch == 1 && !((q0 != ejj || i != k) && (q0 != ss || i != l) && (ii != ejj || j != k) &&
+                                 (ii != ss || j != l)))
+                    continue;
+                my_surv++;
+                if (KIND == 0) {
+                    const double sg = (esg <= floor_sigma) ? 1.0 / sqrtpi : esg;
+                    const double pc = exp(-(delta * delta) / (sg * sg)) /
+                                      (sg * sqrtpi * ((double)nptk * (double)nptk * (double)nptk) *
+                                       (double)(nb * nb * nb * nb));
+                    const int o = (threadIdx.x >> 5) * nb + i;
+                    atomicAdd(&ncnt[o], 1);
+                    atomicAdd(&pacc[o], pc);
+                    continue;
+                }
+                const double w1 = swj[x];
+                if (w1 <= 1.25 || ew2 <= 1.25 || ew3 <= 1.25) continue;  // WP4 = 0 exactly
+                const int pos = atomicAdd(&cnt[idx], 1);
+                if (pos >= p.subcap) {  // cannot happen with the capacity checks
+                    atomicOr(p.err, kErrQueue);
+                    continue;
+                }
+                qbase[(size_t)idx * p.subcap + pos] = epk;
+                qsig[(size_t)idx * p.subcap + pos] = esg;
             }
             ckl += Br;
             cj += Bq;
