@@ -82,8 +82,9 @@ struct Layout {
 // Phase A stages the (v, omega) records of the third phonon's grid points of the
 // next stgp passes, and those of the matching fourth-phonon points, in shared
 // memory (at most kStageSlots points per stage), so that a candidate reads them
-// there instead of from global memory.  stgp divides kCheckEvery, so a stage
-// never straddles a queue flush.
+// there instead of from global memory.  The queues are drained only at a stage
+// boundary, so a stage never straddles a flush; stgp <= kCheckEvery keeps the
+// queue headroom within the capacity the host reserves.
 constexpr int kStageSlots = 32;
 __host__ __device__ inline int stage_passes(int nb2) {
     int P = 8;
@@ -1141,7 +1142,10 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
             swj[rank] = wj_;
             sidx[rank] = (i << 16) | j;  // the pair itself: no division by nb in the window loop
         }
-        if (idx == 0) misc[1] = nvalid;
+        if (idx == 0) {
+            misc[1] = nvalid;
+            misc[2] = 0;  // no bin near its capacity
+        }
         cnt[idx] = 0;
     }
     for (int x = threadIdx.x; x < nb * (KIND == 0 ? kThreads / 32 : 1); x += blockDim.x) {
@@ -1190,14 +1194,19 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
         int4* stgi = reinterpret_cast<int4*>(smem + L.stgi);
         int stage_first = 0;
         for (int base = 0; base < total; base += blockDim.x, iter++) {
-            if (KIND == 2 && (iter % kCheckEvery) == 0) {
-                if (queue_nearly_full(p, cnt, nb2, misc))
+            if ((iter % L.stgp) == 0) {
+                __syncthreads();
+                // Queue capacity: an append that leaves a bin with fewer than stgp passes
+                // of room (one entry per thread and pass) raises misc[2]; at this barrier
+                // every thread sees the flag, and the queues are drained before the next
+                // stgp passes, which cannot then overflow them.
+                if (KIND == 2 && misc[2]) {
                     k4_flush<NT, MIXED, LIST, TC>(p, smem, L, qbase, qsig, qpos, ch, ii, q0, m0, m1, m2, n0, n1, n2,
                                                 my_contr);
-            }
-            if ((iter % L.stgp) == 0) {
+                    __syncthreads();  // every thread has read the flag
+                    if (threadIdx.x == 0) misc[2] = 0;
+                }
                 // stage the points of the next stgp passes: their records, their partners and theirs
-                __syncthreads();
                 stage_first = base / nb2;
                 const int nslot = (min(total, base + L.stgp * (int)blockDim.x) - 1) / nb2 - stage_first + 1;
                 for (int x = threadIdx.x; x < nslot * 2 * nb; x += blockDim.x) {
@@ -1305,6 +1314,7 @@ __device__ __forceinline__ void k4_item(const P4Params& p, unsigned char* smem, 
                 const double w1 = swj[x];
                 if (w1 <= 1.25 || ew2 <= 1.25 || ew3 <= 1.25) continue;  // WP4 = 0 exactly
                 const int pos = atomicAdd(&cnt[idx], 1);
+                if (pos >= p.subcap - L.stgp * (int)blockDim.x) misc[2] = 1;
                 if (pos >= p.subcap) {  // cannot happen with the capacity checks
                     atomicOr(p.err, kErrQueue);
                     continue;
