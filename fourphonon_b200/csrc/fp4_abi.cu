@@ -680,9 +680,21 @@ static int k4_blocks(fp4_ctx* c, int nwork, int kind, int nT) {
     return std::max(1, std::min(nbk, nwork));
 }
 
+// The four-phonon work items of the context's system, or FP4_E_CAPACITY when
+// there are more than the kernels' 32-bit work counter can hand out.
+static int k4_nwork(fp4_ctx* c, int& nwork) {
+    const long long n = k4_work_items(c->S.nlist, c->S.nptk);
+    if (n > kMaxWorkItems)
+        return fp4_fail(c, FP4_E_CAPACITY, "3*nlist*nptk = %lld four-phonon work items, above the limit of %lld", n,
+                        kMaxWorkItems);
+    nwork = (int)n;
+    return FP4_OK;
+}
+
 static int run_np4(fp4_ctx* c, int64_t* n_out[3], double* p_out[3]) {
     const int nm = c->S.nb * c->S.nlist;
-    int r;
+    int r, nwork = 0;
+    if ((r = k4_nwork(c, nwork))) return r;
     if ((r = c->b_out.reserve(c, (size_t)nm * 3 * (sizeof(unsigned long long) + sizeof(double))))) return r;
     if ((r = c->b_work.reserve(c, 64))) return r;
     unsigned long long* dn = c->b_out.as<unsigned long long>();
@@ -693,7 +705,7 @@ static int run_np4(fp4_ctx* c, int64_t* n_out[3], double* p_out[3]) {
     p.S = c->S;
     p.F = DevIfc{};
     p.nT = 1;
-    p.nwork = 3 * c->S.nlist * c->S.nptk;
+    p.nwork = nwork;
     p.work_counter = c->b_work.as<int>();
     p.n_count = dn;
     p.p_sum = dp;
@@ -828,11 +840,11 @@ int fp4_run_rta4(fp4_ctx* c, int nT, const double* temps) {
     const int nm = S.nb * S.nlist;
     const bool mixed = (c->precision != FP4_PREC_FP64);
     size_t sm = k4_smem(2, nT, mixed, S, c->ifc4.F);
-    const int nwork = 3 * S.nlist * S.nptk;
+    int r, nwork = 0;
+    if ((r = k4_nwork(c, nwork))) return r;
     // the queue is sized for the larger of the two grids; the tensor-core plan needs its capacity
     int nblocks = k4_blocks(c, nwork, 2, nT);
     P4Params p{};
-    int r;
     if ((r = k4_queue(c, std::max(nblocks, c->sm_count * k4_tc_ctas_per_sm()), false, p))) return r;
     TcPlan plan{};
     size_t tc_smem = 0;
@@ -975,6 +987,8 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
     size_t sm = k4_smem(3, 1, mixed, S, c->ifc4.F);
     if (sm > 227 * 1024)
         return fp4_fail(c, FP4_E_CAPACITY, "4ph reciprocal cluster table needs %zu B of shared memory (limit 227 KB)", sm);
+    int nwork = 0;
+    if ((r = k4_nwork(c, nwork))) return r;
     const int64_t* N[3] = {n_pp, n_pm, n_mm};
     int64_t* O[3][3] = {{i2pp, i3pp, i4pp}, {i2pm, i3pm, i4pm}, {i2mm, i3mm, i4mm}};
     double* GO[3] = {gamma_pp, gamma_pm, gamma_mm};
@@ -1030,7 +1044,6 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
     if ((r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wb_stride(1) * sizeof(double)))) return r;
     CK(launch_wbose(S, c->b_temps.as<double>(), 1, wb_stride(1), c->b_wb.as<double>(), c->stream));
     c->launches++;
-    const int nwork = 3 * S.nlist * S.nptk;
     const int nblocks = k4_blocks(c, nwork, 3, 1);
     if ((r = k4_queue(c, nblocks, true, p))) return r;
     if ((r = c->b_part.reserve(c, (size_t)nwork * S.nb * 2 * sizeof(double)))) return r;

@@ -9,6 +9,12 @@ namespace fp4 {
 
 constexpr int kQ3 = 2048;  // 3-phonon survivor queue (shared memory entries)
 
+// Four-phonon work items (q, q', channel) of one solve: 3*nlist*nptk.  The kernels
+// index them and hand them out with 32-bit integers, and every CTA fetches once
+// past the last item, so calls with more than kMaxWorkItems are refused.
+constexpr long long kMaxWorkItems = (1LL << 31) - (1LL << 20);
+inline long long k4_work_items(int nlist, int nptk) { return 3LL * nlist * nptk; }
+
 struct P3Params {
     DevSys S;
     DevIfc F;

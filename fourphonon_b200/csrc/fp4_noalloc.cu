@@ -144,6 +144,7 @@ extern "C" int fp4_np_driver_4ph_noalloc(const fp4_globals* g, const double* ene
     if (g->natoms < 1 || g->nbands != 3 * g->natoms || g->nbands > kMaxNb) return FP4_E_ARG;
     const int nptk = g->ngrid[0] * g->ngrid[1] * g->ngrid[2], nb = g->nbands;
     if (nlist < 1 || nlist > nptk) return FP4_E_ARG;
+    if (k4_work_items(nlist, nptk) > kMaxWorkItems) return FP4_E_CAPACITY;
     const int nm = nb * nlist;
     // scratch layout
     const size_t o_wv = 0;
@@ -200,7 +201,7 @@ extern "C" int fp4_np_driver_4ph_noalloc(const fp4_globals* g, const double* ene
     S.list0 = list0;
     p.F = DevIfc{};
     p.nT = 1;
-    p.nwork = 3 * nlist * nptk;
+    p.nwork = (int)k4_work_items(nlist, nptk);
     p.work_counter = misc;
     p.n_count = cnt;
     p.p_sum = ps;

@@ -292,7 +292,10 @@ extern "C" int fp4_server_admit(fp4_server* srv, const fp4_globals* g, const dou
         (r = sl.result.reserve(c, (size_t)(S.nb + 1) * 9 * sizeof(double))))
         return pass(r);
     // Bose factors at T, partial sums, outputs
-    const int nwork = 3 * nlist * S.nptk;
+    if (k4_work_items(nlist, S.nptk) > kMaxWorkItems)
+        return sfail(srv, FP4_E_CAPACITY, "3*nlist*nptk = %lld four-phonon work items, above the limit of %lld",
+                     k4_work_items(nlist, S.nptk), kMaxWorkItems);
+    const int nwork = (int)k4_work_items(nlist, S.nptk);
     if ((r = c->b_temps.upload(c, &g->T, sizeof(double))) ||
         (r = c->b_wb.reserve(c, (size_t)S.nptk * S.nb * wb_stride(1) * sizeof(double))) ||
         (r = c->b_part.reserve(c, (size_t)nwork * S.nb * 2 * sizeof(double))) ||

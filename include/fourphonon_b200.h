@@ -22,6 +22,10 @@
  * one context are not re-entrant (the reference calls them from the MPI main
  * thread); distinct contexts are independent.  All arrays are caller-owned
  * host memory; device copies are owned by the context.
+ *
+ * Limits: ngrid(d) <= 64, nbands <= 32, up to 8 temperatures in one call, and
+ * for the four-phonon drivers 3*nlist*nptk < 2^31 - 2^20 work items (q, q',
+ * channel); larger calls return FP4_E_ARG or FP4_E_CAPACITY.
  */
 #ifndef FOURPHONON_B200_H
 #define FOURPHONON_B200_H
