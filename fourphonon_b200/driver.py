@@ -149,6 +149,7 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
     os.makedirs(outdir, exist_ok=True)
     own = ctx is None
     ctx = ctx or abi.Context(0)
+    files = []
     try:
         n3 = ctx.np_driver(s)
         n4 = p4 = None
@@ -164,6 +165,7 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
         results = []
         f303 = open(os.path.join(outdir, "BTE.KappaTensorVsT_RTA"), "w")
         f403 = open(os.path.join(outdir, "BTE.KappaTensorVsT_CONV"), "w") if convergence else None
+        files += [f for f in (f303, f403) if f is not None]
         for t, T in enumerate(s.temperatures):
             tdir = os.path.join(outdir, f"T{int(round(T))}K")
             os.makedirs(tdir, exist_ok=True)
@@ -204,7 +206,7 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
             kap = ctx.tconduct(s, F, T=T).reshape(3, 3, s.nb)  # [d2][d1][branch]
             kb = np.stack([symmetrize_tensor(s, kap[:, :, b].T) for b in range(s.nb)])  # (nb,3,3)
             ktot = kb.sum(axis=0)
-            kappa_lines = [f"{0:9d}" + "".join(fortran_e(x, 20, 10) for x in kb.transpose(0, 1, 2).ravel(order="F"))]
+            kappa_lines = [f"{0:9d}" + "".join(fortran_e(x, 20, 10) for x in kb.ravel(order="F"))]
             tensor_lines = [f"{0:9d}" + "".join(fortran_e(x, 20, 10) for x in ktot.ravel(order="F"))]
             scalar_lines = [f"{0:9d}" + fortran_e(np.trace(ktot) / 3.0, 20, 10)]
             f303.write(f"{T:7.1f}" + "".join(fortran_e(x, 14, 5) for x in ktot.ravel(order="F")) + "\n")
@@ -233,10 +235,9 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
             _rows(os.path.join(tdir, "BTE.kappa_tensor"), tensor_lines)
             _rows(os.path.join(tdir, "BTE.kappa_scalar"), scalar_lines)
             results.append(res)
-        f303.close()
-        if f403:
-            f403.close()
         return results
     finally:
+        for f in files:
+            f.close()
         if own:
             ctx.close()
