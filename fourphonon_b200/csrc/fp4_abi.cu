@@ -491,6 +491,7 @@ int fp4_launch_rta3(fp4_ctx* c, const fp4_globals* g, double* d_out) {
 extern "C" int fp4_np_driver(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
                              int32_t nlist, const int32_t* list, const int32_t* ijk, int32_t* n_plus,
                              double* p_plus, int32_t* n_minus, double* p_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_plus || !n_minus || !p_plus || !p_minus) return fp4_fail(c, FP4_E_ARG, "null output");
     int r;
@@ -523,6 +524,7 @@ extern "C" int fp4_ind_only_driver(fp4_ctx* c, const fp4_globals* g, const doubl
                                    int32_t nlist, const int32_t* list, const int32_t* ijk, const int32_t* n_plus,
                                    const int32_t* n_minus, int32_t* ind2_plus, int32_t* ind3_plus, int32_t* ind2_minus,
                                    int32_t* ind3_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_plus || !n_minus) return fp4_fail(c, FP4_E_ARG, "null N_plus/N_minus");
     int r;
@@ -571,6 +573,7 @@ extern "C" int fp4_rta_driver(fp4_ctx* c, const fp4_globals* g, const double* en
                               int32_t ntri, const double* phi, const double* r_j, const double* r_k,
                               const int32_t* index_i, const int32_t* index_j, const int32_t* index_k, double* rate,
                               double* rate_plus, double* rate_minus, double* wp3_plus, double* wp3_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!rate || !rate_plus || !rate_minus || !wp3_plus || !wp3_minus) return fp4_fail(c, FP4_E_ARG, "null output");
     if (!eigenvect) return fp4_fail(c, FP4_E_ARG, "null eigenvect");
@@ -606,6 +609,7 @@ extern "C" int fp4_ind_driver(fp4_ctx* c, const fp4_globals* g, const double* en
                               const int32_t* index_k, int32_t* ind2_plus, int32_t* ind3_plus, double* gamma_plus,
                               int32_t* ind2_minus, int32_t* ind3_minus, double* gamma_minus, double* rate,
                               double* rate_plus, double* rate_minus, double* wp3_plus, double* wp3_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_plus || !n_minus || !rate || !rate_plus || !rate_minus || !wp3_plus || !wp3_minus || !eigenvect)
         return fp4_fail(c, FP4_E_ARG, "null argument");
@@ -732,6 +736,7 @@ static int run_np4(fp4_ctx* c, int64_t* n_out[3], double* p_out[3]) {
 extern "C" int fp4_np_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double* energy, const double* velocity,
                                  int32_t nlist, const int32_t* list, const int32_t* ijk, int64_t* n_pp, double* p_pp,
                                  int64_t* n_pm, double* p_pm, int64_t* n_mm, double* p_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_pp || !n_pm || !n_mm || !p_pp || !p_pm || !p_mm) return fp4_fail(c, FP4_E_ARG, "null output");
     int r;
@@ -746,6 +751,7 @@ extern "C" int fp4_ind_only_driver_4ph(fp4_ctx* c, const fp4_globals* g, const d
                                        const int64_t* n_pp, const int64_t* n_pm, const int64_t* n_mm, int64_t* i2pp,
                                        int64_t* i3pp, int64_t* i4pp, int64_t* i2pm, int64_t* i3pm, int64_t* i4pm,
                                        int64_t* i2mm, int64_t* i3mm, int64_t* i4mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_pp || !n_pm || !n_mm) return fp4_fail(c, FP4_E_ARG, "null counts");
     int r;
@@ -906,6 +912,7 @@ extern "C" int fp4_rta_driver_4ph_multi_t(fp4_ctx* c, const fp4_globals* g, int3
                                           const int32_t* index_i, const int32_t* index_j, const int32_t* index_k,
                                           const int32_t* index_l, double* rate_pp, double* rate_pm, double* rate_mm,
                                           double* wp_pp, double* wp_pm, double* wp_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!temperatures || !rate_pp || !rate_pm || !rate_mm || !wp_pp || !wp_pm || !wp_mm || !eigenvect)
         return fp4_fail(c, FP4_E_ARG, "null argument");
@@ -974,6 +981,7 @@ extern "C" int fp4_ind_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
                                   int64_t* i2mm, int64_t* i3mm, int64_t* i4mm, double* gamma_mm, double* rate_4ph,
                                   double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp, double* wp_pm,
                                   double* wp_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!g || !n_pp || !n_pm || !n_mm || !rate_4ph || !rate_pp || !rate_pm || !rate_mm || !wp_pp || !wp_pm ||
         !wp_mm || !eigenvect)
@@ -1091,6 +1099,7 @@ extern "C" int fp4_rta_driver_4ph(fp4_ctx* c, const fp4_globals* g, const double
                                   const double* r_l, const int32_t* index_i, const int32_t* index_j,
                                   const int32_t* index_k, const int32_t* index_l, double* rate_4ph, double* rate_pp,
                                   double* rate_pm, double* rate_mm, double* wp_pp, double* wp_pm, double* wp_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!g || !rate_4ph) return fp4_fail(c, FP4_E_ARG, "null argument");
     int r = fp4_rta_driver_4ph_multi_t(c, g, 1, &g->T, energy, velocity, eigenvect, nlist, list, ijk, ntri, psi, r_j,

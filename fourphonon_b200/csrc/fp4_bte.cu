@@ -382,6 +382,7 @@ static int check_g(fp4_ctx* c, const fp4_globals* g) {
 extern "C" int fp4_iteration0(fp4_ctx* c, const fp4_globals* g, int32_t nlist, const int32_t* nequi,
                               const int32_t* allequi, int32_t nsr, const double* omega, const double* velocity,
                               const double* tau_zero, double* f_n) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     int r;
     if ((r = check_g(c, g))) return r;
@@ -588,6 +589,7 @@ extern "C" int fp4_iteration(fp4_ctx* c, const fp4_globals* g, int32_t nlist, co
                              int32_t ntotal_plus, int32_t ntotal_minus, const int32_t* i2p, const int32_t* i3p,
                              const int32_t* i2m, const int32_t* i3m, const double* omega, const double* velocity,
                              const double* gp, const double* gm, const double* tau_zero, double* f_n) {
+    FP4_TRACE();
     return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
                      ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, nullptr);
 }
@@ -599,6 +601,7 @@ extern "C" int fp4_iteration_jacobi(fp4_ctx* c, const fp4_globals* g, int32_t nl
                                     const int32_t* i2p, const int32_t* i3p, const int32_t* i2m, const int32_t* i3m,
                                     const double* omega, const double* velocity, const double* gp, const double* gm,
                                     const double* tau_zero, double* f_n) {
+    FP4_TRACE();
     return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
                      ntotal_minus, i2p, i3p, i2m, i3m, omega, velocity, gp, gm, tau_zero, f_n, nullptr, true);
 }
@@ -614,6 +617,7 @@ extern "C" int fp4_iteration_4ph(fp4_ctx* c, const fp4_globals* g, int32_t nlist
                                  const int64_t* i2mm, const int64_t* i3mm, const int64_t* i4mm, const double* omega,
                                  const double* velocity, const double* gp, const double* gm, const double* gpp,
                                  const double* gpm, const double* gmm, const double* tau_zero, double* f_n) {
+    FP4_TRACE();
     Lists4 l4{{n_pp, n_pm, n_mm}, {ntotal_pp, ntotal_pm, ntotal_mm}, {i2pp, i2pm, i2mm}, {i3pp, i3pm, i3mm},
               {i4pp, i4pm, i4mm}, {gpp, gpm, gmm}};
     return run_sweep(c, g, nlist, nequi, allequi, typeofsym, nsr, id_equi, symmetrizers, n_plus, n_minus, ntotal_plus,
@@ -621,6 +625,7 @@ extern "C" int fp4_iteration_4ph(fp4_ctx* c, const fp4_globals* g, int32_t nlist
 }
 
 extern "C" int fp4_symmetrize_fn(fp4_ctx* c, const fp4_globals* g, const double* symmetrizers, double* f_n) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     int r;
     if ((r = check_g(c, g))) return r;
@@ -641,6 +646,7 @@ extern "C" int fp4_symmetrize_fn(fp4_ctx* c, const fp4_globals* g, const double*
 
 extern "C" int fp4_tconduct(fp4_ctx* c, const fp4_globals* g, double V, const double* omega, const double* velocity,
                             const double* f_n, double* kappa, double* kmode) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     int r;
     if ((r = check_g(c, g))) return r;
@@ -717,11 +723,13 @@ static int run_cumulative(fp4_ctx* c, const fp4_globals* g, double V, const doub
 extern "C" int fp4_cumulative_tconduct(fp4_ctx* c, const fp4_globals* g, double V, const double* omega,
                                        const double* velocity, const double* f_n, int32_t nticks, double* ticks,
                                        double* results) {
+    FP4_TRACE();
     return run_cumulative(c, g, V, omega, velocity, f_n, nticks, ticks, results, 0);
 }
 
 extern "C" int fp4_cumulative_tconduct_omega(fp4_ctx* c, const fp4_globals* g, double V, const double* omega,
                                              const double* velocity, const double* f_n, int32_t nticks,
                                              double* ticks, double* results) {
+    FP4_TRACE();
     return run_cumulative(c, g, V, omega, velocity, f_n, nticks, ticks, results, 1);
 }

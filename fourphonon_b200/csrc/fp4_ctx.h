@@ -7,10 +7,23 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fourphonon_b200.h"
 #include "fp4_device.cuh"
 
 struct fp4_ctx;
+
+// An NVTX range over one C-ABI call, named after the entry point: a CUDA
+// profiler's timeline then shows which call launched which kernels.  Without a
+// profiler attached the push and pop do nothing.
+struct Fp4Trace {
+    explicit Fp4Trace(const char* name) { nvtxRangePushA(name); }
+    ~Fp4Trace() { nvtxRangePop(); }
+    Fp4Trace(const Fp4Trace&) = delete;
+    Fp4Trace& operator=(const Fp4Trace&) = delete;
+};
+#define FP4_TRACE() Fp4Trace fp4_trace_range_(__func__)
 
 // Grow-only device buffer that remembers a hash of the bytes last uploaded,
 // so repeated calls with unchanged inputs skip the host-to-device copy.

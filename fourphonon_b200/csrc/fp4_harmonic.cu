@@ -303,6 +303,7 @@ extern "C" int fp4_eigen_dm(fp4_ctx* c, const fp4_globals* g, const double* latt
                             const int32_t scell[3], const double* fc, int32_t nonanalytic, const double* epsilon,
                             const double* born, double V, const double* symmetrizers, double* omega,
                             double* velocity, double* eigenvect) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!g || !lattvec || !cartesian || !scell || !fc || !symmetrizers || !omega || !velocity || !eigenvect)
         return fp4_fail(c, FP4_E_ARG, "null argument");

@@ -624,6 +624,7 @@ extern "C" int fp4_np_driver_4ph_sample(fp4_ctx* c, const fp4_globals* g, const 
                                         const double* velocity, int32_t nlist, const int32_t* list,
                                         const int32_t* ijk, int64_t nsamples, uint64_t seed, int64_t* n_pp,
                                         double* p_pp, int64_t* n_pm, double* p_pm, int64_t* n_mm, double* p_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_pp || !n_pm || !n_mm || !p_pp || !p_pm || !p_mm) return fp4_fail(c, FP4_E_ARG, "null output");
     int r;
@@ -655,6 +656,7 @@ extern "C" int fp4_rta_driver_4ph_sample_multi_t(fp4_ctx* c, const fp4_globals* 
                                                  const int32_t* index_k, const int32_t* index_l, int64_t nsamples,
                                                  uint64_t seed, double* rate_pp, double* rate_pm, double* rate_mm,
                                                  double* wp_pp, double* wp_pm, double* wp_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!temperatures || !rate_pp || !rate_pm || !rate_mm || !wp_pp || !wp_pm || !wp_mm || !eigenvect)
         return fp4_fail(c, FP4_E_ARG, "null argument");
@@ -687,6 +689,7 @@ extern "C" int fp4_rta_driver_4ph_sample(fp4_ctx* c, const fp4_globals* g, const
                                          const int32_t* index_l, int64_t nsamples, uint64_t seed, double* rate_4ph,
                                          double* rate_pp, double* rate_pm, double* rate_mm, double* wp_pp,
                                          double* wp_pm, double* wp_mm) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!g || !rate_4ph) return fp4_fail(c, FP4_E_ARG, "null argument");
     int r = fp4_rta_driver_4ph_sample_multi_t(c, g, 1, &g->T, energy, velocity, eigenvect, nlist, list, ijk, ntri, psi,
@@ -742,6 +745,7 @@ extern "C" int fp4_np_driver_sample(fp4_ctx* c, const fp4_globals* g, const doub
                                     int32_t nlist, const int32_t* list, const int32_t* ijk, int64_t nsamples,
                                     uint64_t seed, int32_t* n_plus, double* p_plus, int32_t* n_minus,
                                     double* p_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!n_plus || !p_plus || !n_minus || !p_minus) return fp4_fail(c, FP4_E_ARG, "null output");
     int r;
@@ -775,6 +779,7 @@ extern "C" int fp4_rta_driver_sample(fp4_ctx* c, const fp4_globals* g, const dou
                                      const int32_t* index_i, const int32_t* index_j, const int32_t* index_k,
                                      int64_t nsamples, uint64_t seed, double* rate, double* rate_plus,
                                      double* rate_minus, double* wp3_plus, double* wp3_minus) {
+    FP4_TRACE();
     if (!c) return FP4_E_ARG;
     if (!rate || !rate_plus || !rate_minus || !wp3_plus || !wp3_minus) return fp4_fail(c, FP4_E_ARG, "null output");
     if (!eigenvect) return fp4_fail(c, FP4_E_ARG, "null eigenvect");

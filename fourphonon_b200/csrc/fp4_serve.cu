@@ -235,6 +235,7 @@ extern "C" int fp4_server_admit(fp4_server* srv, const fp4_globals* g, const dou
                                 const int32_t* index_k4, const int32_t* index_l4, int32_t nsymm_rot,
                                 const int32_t* nequi, const int32_t* allequilist, const double* crotations,
                                 double volume, int32_t* slot_out) {
+    FP4_TRACE();
     if (!srv) return FP4_E_ARG;
     if (!g || !slot_out || !nequi || !allequilist || !crotations || !energy || !velocity || !eigenvect || nsymm_rot < 1)
         return sfail(srv, FP4_E_ARG, "null argument");
@@ -364,6 +365,7 @@ static int finish_slot(fp4_server* srv, Slot& sl) {
 }
 
 extern "C" int fp4_server_tick(fp4_server* srv, int64_t max_items, int32_t* finished, int32_t* nfinished) {
+    FP4_TRACE();
     if (!srv) return FP4_E_ARG;
     if (!finished || !nfinished || max_items < 1) return sfail(srv, FP4_E_ARG, "bad argument");
     *nfinished = 0;
@@ -429,6 +431,7 @@ extern "C" int fp4_server_tick(fp4_server* srv, int64_t max_items, int32_t* fini
 extern "C" int fp4_server_collect(fp4_server* srv, int32_t slot, double* rate3_plus, double* rate3_minus,
                                   double* rate4_pp, double* rate4_pm, double* rate4_mm, double* kappa_branch,
                                   double* kappa, int64_t* n_processes) {
+    FP4_TRACE();
     if (!srv) return FP4_E_ARG;
     if (slot < 0 || slot >= srv->max_slots || srv->slots[slot].state != Slot::DONE)
         return sfail(srv, FP4_E_STATE, "slot %d holds no finished solve", slot);

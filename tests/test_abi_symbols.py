@@ -38,3 +38,18 @@ def test_create_without_device_fails_cleanly():
         lib.fp4_destroy(h)
         pytest.skip("a CUDA device is present")
     assert rc in (-1, -2)
+
+
+def test_null_context_is_refused():
+    """Entry points called with a null context return FP4_E_ARG (after opening and
+    closing their NVTX range, which does nothing without a profiler)."""
+    lib = abi.load()
+    f = lib.fp4_iteration0
+    f.restype = ct.c_int
+    f.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_int32, ct.c_void_p,
+                  ct.c_void_p, ct.c_void_p, ct.c_void_p]
+    assert f(None, None, 0, None, None, 0, None, None, None, None) == abi.FP4_E_ARG
+    t = lib.fp4_server_tick
+    t.restype = ct.c_int
+    t.argtypes = [ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p]
+    assert t(None, 1, None, None) == abi.FP4_E_ARG
