@@ -13,6 +13,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "libfp4_oracle.so")
+# FP4_ORACLE_LIB names another build of the same source (the sanitizer build of
+# `make sanitize`); it is used as it is, without the rebuild check below.
+_LIB_OVERRIDE = os.environ.get("FP4_ORACLE_LIB")
 _lib = None
 
 
@@ -37,9 +40,13 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "fp4_oracle.c")):
-            build()
-        _lib = ct.CDLL(_LIB)
+        if _LIB_OVERRIDE:
+            _lib = ct.CDLL(_LIB_OVERRIDE)
+        else:
+            if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(
+                    os.path.join(_HERE, "fp4_oracle.c")):
+                build()
+            _lib = ct.CDLL(_LIB)
         _lib.fp4o_base_sigma.restype = ct.c_double
         _lib.fp4o_ind_only3.restype = ct.c_int64
         _lib.fp4o_ind_only4.restype = ct.c_int64
