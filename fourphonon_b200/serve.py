@@ -15,6 +15,7 @@ and the solves/s of the whole stream.
 from __future__ import annotations
 
 import ctypes as ct
+import json
 import time
 from dataclasses import dataclass, field
 
@@ -151,13 +152,17 @@ class Request:
 
 
 def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_counter, sleep=time.sleep,
-               target_tick_ms=None, max_tick_items=1 << 22):
+               target_tick_ms=None, max_tick_items=1 << 22, metrics=None):
     """Serve `requests` (sorted by arrival) on the wall clock; returns them with
     admission/finish times and results, plus a summary dict.
 
     With target_tick_ms, the number of work items per tick follows the last
     tick's device time so that a tick lasts about that long: long enough to
-    hide the per-tick host work, short enough to admit new requests often."""
+    hide the per-tick host work, short enough to admit new requests often.
+
+    metrics: a writable text stream that receives one JSON line per finished
+    request (tag, arrival, admission and finish times, latency, processes) as
+    it finishes, and one line with the summary at the end."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     waiting = []
     running = {}
@@ -191,6 +196,10 @@ def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_cou
                 r.result = server.collect(slot)
                 t_collect += clock() - tc
                 r.finished = clock() - t0
+                if metrics is not None:
+                    _emit(metrics, event="request", tag=_plain(r.tag), arrival_s=r.arrival, admitted_s=r.admitted,
+                          finished_s=r.finished, latency_ms=1e3 * r.latency,
+                          processes=int(r.result.get("n_processes", 0)))
             ticks += 1
             if target_tick_ms:
                 ms = server.status()["last_tick_ms"] if hasattr(server, "status") else 0.0
@@ -206,4 +215,15 @@ def run_stream(server: Server, requests, tick_items=200_000, clock=time.perf_cou
                    processes=int(sum(r.result.get("n_processes", 0) for r in reqs)),
                    host_s={"admit": t_admit, "tick": t_tick, "collect": t_collect})
     summary["processes_per_s"] = summary["processes"] / wall if wall > 0 else 0.0
+    if metrics is not None:
+        _emit(metrics, event="summary", **summary)
     return reqs, summary
+
+
+def _plain(x):
+    return x if isinstance(x, (int, float, str, bool)) or x is None else str(x)
+
+
+def _emit(stream, **fields):
+    stream.write(json.dumps(fields) + "\n")
+    stream.flush()

@@ -97,3 +97,24 @@ def test_budget_blocks_until_collect():
     adm = sorted(r.admitted for r in done)
     assert adm[1] >= fin[0] and adm[2] >= fin[1]
     assert all(len(t) == 1 for t in srv.tick_log)
+
+
+def test_metrics_stream():
+    import io
+    import json
+
+    clk = FakeClock()
+    srv = FakeServer(clk, slots=2, budget=10)
+    reqs = [serve.Request(0.001 * i, FakeSolve(10 + i, 3), 300.0, tag=i) for i in range(4)]
+    out = io.StringIO()
+    done, summary = serve.run_stream(srv, reqs, tick_items=4, clock=clk, sleep=clk.sleep, metrics=out)
+    lines = [json.loads(x) for x in out.getvalue().splitlines()]
+    assert [x["event"] for x in lines] == ["request"] * 4 + ["summary"]
+    by = {r.tag: r for r in done}
+    for x in lines[:-1]:
+        r = by[x["tag"]]
+        assert x["finished_s"] == r.finished and x["admitted_s"] == r.admitted
+        assert abs(x["latency_ms"] - 1e3 * r.latency) < 1e-9
+        assert x["processes"] == r.solve.work
+    assert [x["finished_s"] for x in lines[:-1]] == sorted(x["finished_s"] for x in lines[:-1])
+    assert lines[-1]["p99_ms"] == summary["p99_ms"] and lines[-1]["requests"] == 4
