@@ -21,8 +21,10 @@ E14.5, F7.1, I9, I0), so the files read the same way.
 """
 from __future__ import annotations
 
+import json
 import math
 import os
+import time
 
 import numpy as np
 
@@ -144,24 +146,45 @@ def write_final(tdir, s, F, ctx, T, nticks=100):
 
 
 def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(np.float32(1e-5)),
-        ctx=None, log=print, four_phonon_iteration=False):
-    """The hot-path section of ShengBTE for solve `s`; returns per-T results."""
+        ctx=None, log=print, four_phonon_iteration=False, metrics=None):
+    """The hot-path section of ShengBTE for solve `s`; returns per-T results.
+
+    metrics: a writable text stream that receives one JSON line per stage
+    (counting, rates, the BTE loop, the output files) with its wall-clock
+    seconds, and the temperature and process counts where they apply; the
+    reference prints MPI_Wtime differences around the same stages."""
     os.makedirs(outdir, exist_ok=True)
     own = ctx is None
     ctx = ctx or abi.Context(0)
     files = []
+
+    def stage(name, t0, **fields):
+        if metrics is not None:
+            metrics.write(json.dumps({"event": "stage", "stage": name, "seconds": time.perf_counter() - t0,
+                                      **fields}) + "\n")
+            metrics.flush()
+
     try:
+        t0 = time.perf_counter()
         n3 = ctx.np_driver(s)
+        stage("np_driver", t0, processes=int(n3[0].sum()) + int(n3[1].sum()))
         n4 = p4 = None
         if four_phonon:
+            t0 = time.perf_counter()
             n4, p4 = ctx.np_driver_4ph(s)
+            stage("np_driver_4ph", t0, processes=int(sum(int(x.sum()) for x in n4)))
         write_counts(outdir, s, (n3[0], n3[1]), (n3[2], n3[3]), n4, p4)
         log(f"Info: Ntotal_plus = {int(n3[0].sum())}  Ntotal_minus = {int(n3[1].sum())}")
         if four_phonon:
             log(f"Info: Ntotal_plusplus,Ntotal_plusminus,Ntotal_minusminus= "
                 f"{int(n4[0].sum())} {int(n4[1].sum())} {int(n4[2].sum())}")
         it4 = four_phonon and four_phonon_iteration and convergence
-        r4 = ctx.rta_driver_4ph(s) if four_phonon and not it4 else None
+        r4 = None
+        if four_phonon and not it4:
+            t0 = time.perf_counter()
+            r4 = ctx.rta_driver_4ph(s)
+            stage("rta_driver_4ph", t0, temperatures=[float(x) for x in s.temperatures],
+                  processes=int(sum(int(x.sum()) for x in n4)))
         results = []
         f303 = open(os.path.join(outdir, "BTE.KappaTensorVsT_RTA"), "w")
         f403 = open(os.path.join(outdir, "BTE.KappaTensorVsT_CONV"), "w") if convergence else None
@@ -169,11 +192,14 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
         for t, T in enumerate(s.temperatures):
             tdir = os.path.join(outdir, f"T{int(round(T))}K")
             os.makedirs(tdir, exist_ok=True)
+            t0 = time.perf_counter()
             if convergence:
                 lists = ctx.ind_driver(s, n3[0], n3[1], T=T)
                 r3 = lists
             else:
                 r3 = ctx.rta_driver(s, T=T)
+            stage("ind_driver" if convergence else "rta_driver", t0, T=float(T),
+                  processes=int(n3[0].sum()) + int(n3[1].sum()))
             rate3 = r3["rate_plus"] + r3["rate_minus"]
             _rows(os.path.join(tdir, "BTE.w_3ph"), _mode_lines(s, rate3))
             _rows(os.path.join(tdir, "BTE.w_3ph_plus"), _mode_lines(s, r3["rate_plus"]))
@@ -185,7 +211,9 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
             ind4 = None
             if four_phonon:
                 if it4:
+                    t0 = time.perf_counter()
                     ind4 = ctx.ind_driver_4ph(s, n4[0], n4[1], n4[2], T=T)
+                    stage("ind_driver_4ph", t0, T=float(T), processes=int(sum(int(x.sum()) for x in n4)))
                     rates = [ind4["rate_pp"], ind4["rate_pm"], ind4["rate_mm"]]
                     wps = [ind4["wp_pp"], ind4["wp_pm"], ind4["wp_mm"]]
                 else:
@@ -202,6 +230,7 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
             tau = np.zeros_like(rate)
             nz = rate != 0
             tau[nz] = 1.0 / rate[nz]
+            t0 = time.perf_counter()
             F = ctx.iteration0(s, tau)
             kap = ctx.tconduct(s, F, T=T).reshape(3, 3, s.nb)  # [d2][d1][branch]
             kb = np.stack([symmetrize_tensor(s, kap[:, :, b].T) for b in range(s.nb)])  # (nb,3,3)
@@ -211,7 +240,9 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
             scalar_lines = [f"{0:9d}" + fortran_e(np.trace(ktot) / 3.0, 20, 10)]
             f303.write(f"{T:7.1f}" + "".join(fortran_e(x, 14, 5) for x in ktot.ravel(order="F")) + "\n")
             res = {"T": T, "kappa_rta": ktot.copy(), "rate3": rate3, "rate4": rate4}
+            stage("kappa_rta", t0, T=float(T))
             if convergence:
+                t0 = time.perf_counter()
                 it = 0
                 for it in range(1, maxiter + 1):
                     kold = ktot.copy()
@@ -230,10 +261,13 @@ def run(s, outdir, convergence=True, four_phonon=True, maxiter=1000, eps=float(n
                 f403.write(f"{T:7.1f}" + "".join(fortran_e(x, 14, 5) for x in ktot.ravel(order="F")) + f"{it:6d}\n")
                 res["kappa_conv"] = ktot.copy()
                 res["iterations"] = it
+                stage("iterations", t0, T=float(T), iterations=int(it))
+            t0 = time.perf_counter()
             write_final(tdir, s, F, ctx, T)
             _rows(os.path.join(tdir, "BTE.kappa"), kappa_lines)
             _rows(os.path.join(tdir, "BTE.kappa_tensor"), tensor_lines)
             _rows(os.path.join(tdir, "BTE.kappa_scalar"), scalar_lines)
+            stage("outputs", t0, T=float(T))
             results.append(res)
         return results
     finally:
