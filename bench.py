@@ -201,7 +201,7 @@ def dist_setup(n):
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -278,9 +278,13 @@ def cpu_sample(s, target_s=15.0, full=False):
 
 
 def run_reference(args):
-    world, rank, local = dist_setup(args.gpus)
-    if rank != 0:
+    # rank 0 alone times the CPU oracle; the other ranks have no work and need no process group
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # torchrun sets OMP_NUM_THREADS=1 for every rank; the one rank that works here takes
+        # every host thread (read when the oracle's OpenMP runtime loads, below)
+        os.environ["OMP_NUM_THREADS"] = str(len(os.sched_getaffinity(0)))
     cfg = config_of(args)
     s = workload(cfg)
     full = args.config == 0
@@ -548,6 +552,9 @@ def run_ours(args):
     ctx.close()
     if rank != 0:
         barrier(world)
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
         return 0
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k4_work_diamond16.txt")
