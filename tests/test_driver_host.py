@@ -145,3 +145,22 @@ def test_driver_sequence_files_and_metrics(tmp_path, cell, it4):
     its = [e for e in events if e["stage"] == "iterations"]
     assert [e["iterations"] for e in its] == [r["iterations"] for r in res]
     assert names.count("outputs") == len(s.temperatures)
+
+
+def test_driver_rta_only_three_phonon(tmp_path, cell):
+    """convergence=.false. and four_phonon=.false.: RTA_driver per temperature,
+    no BTE loop, no four-phonon files and no KappaTensorVsT_CONV."""
+    s = cell
+    res = driver.run(s, str(tmp_path), convergence=False, four_phonon=False, ctx=OracleContext(s),
+                     log=lambda *a: None)
+    for t, T in enumerate(s.temperatures):
+        o = O.Oracle(s, T=T)
+        r3 = o.rta3()
+        assert np.array_equal(res[t]["rate3"], r3[0] + r3[1])
+        assert not res[t]["rate4"].any()
+        assert "kappa_conv" not in res[t]
+        tdir = os.path.join(str(tmp_path), f"T{int(T)}K")
+        assert not os.path.exists(os.path.join(tdir, "BTE.w_4ph"))
+        assert len(open(os.path.join(tdir, "BTE.kappa_scalar")).read().splitlines()) == 1
+    assert not os.path.exists(os.path.join(str(tmp_path), "BTE.KappaTensorVsT_CONV"))
+    assert len(open(os.path.join(str(tmp_path), "BTE.KappaTensorVsT_RTA")).read().splitlines()) == 2
