@@ -33,7 +33,8 @@ namespace fp4 {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kCheckEvery = 8;  // phase-A iterations between queue-capacity checks
+constexpr int kCheckEvery = 8;  // list mode: passes between queue-capacity checks; also the most passes
+                                 // in a phase-A stage (the queues are drained at stage boundaries)
 // Resident persistent CTAs per SM, which sets the register budget.  Three CTAs
 // (80 registers) suit the FP32 contraction of one or two temperatures (1.21x
 // faster than two CTAs on the 16^3 diamond workload) and the counting kernel.
