@@ -717,6 +717,10 @@ def run_serving(args, precision=None, tick_ms=25.0, max_slots=16):
             "arrivals": "Poisson at twice the serial FP64 rate of the prefix",
             "prefix": [{"natoms": na, "grid": g, "T": round(T, 1)} for (na, g, T, sd) in specs],
             "full_stream_estimate_gpu_hours": full_hours, "prefix_estimate_serial_s": acc,
+            "estimate_note": "system.request_seconds leaves out the growth of the contraction with the number "
+                             "of displacement classes and underestimates many-atom cells (compare "
+                             "prefix_estimate_serial_s with the measured serial time of the prefix)",
+            "prefix_serial_fp64_s": sum(times),
             "workload": "seeded stream of 512 random 2-8 atom cells (masses U[6,120] amu, BvK + Gaussian IFCs), "
                         "grids {6,8,10,12,14}^3, T~U[100,1000] K, 3ph+4ph RTA + kappa; the first `requests` of it"}
 

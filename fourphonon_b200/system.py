@@ -248,7 +248,11 @@ def request_seconds(natoms, grid, nlist=None):
     per candidate slot plus the contraction per surviving process, whose number
     grows as nbands^4 (the windows of the nbands^2 sorted pair sums fill up).
     Constants from the 16^3 diamond workload (1.6e-11 s per slot, 2.2 % of
-    nptk^2 nlist nbands^4 survive, 9e-11 s per survivor)."""
+    nptk^2 nlist nbands^4 survive, 9e-11 s per survivor).  The contraction's
+    cost per survivor also grows with the number of displacement classes,
+    which this leaves out, so it underestimates many-atom cells: the first
+    five requests of config4_stream come to 45 s here and took 185 s on a
+    B200, one at a time in FP64."""
     nptk = grid ** 3
     nl = nlist if nlist is not None else nptk // 2 + 4
     nb = 3 * natoms
