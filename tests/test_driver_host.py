@@ -164,3 +164,38 @@ def test_driver_rta_only_three_phonon(tmp_path, cell):
         assert len(open(os.path.join(tdir, "BTE.kappa_scalar")).read().splitlines()) == 1
     assert not os.path.exists(os.path.join(str(tmp_path), "BTE.KappaTensorVsT_CONV"))
     assert len(open(os.path.join(str(tmp_path), "BTE.KappaTensorVsT_RTA")).read().splitlines()) == 2
+
+
+def test_input_directory_to_outputs(tmp_path):
+    """A FourPhonon input directory (CONTROL, FORCE_CONSTANTS_2ND/3RD/4TH) through
+    system.load_inputs (numpy harmonic stage) and driver.run to the BTE.* files,
+    as a user runs it; the rates come from the oracle here, from the device in
+    production."""
+    from fourphonon_b200 import crystal as C
+    from fourphonon_b200 import ifcgen as G
+    from fourphonon_b200 import inputs as I
+    from fourphonon_b200 import system as S
+
+    cr = C.diamond(5.43, (28.085, 28.085))
+    cr.scell = (3, 3, 3)
+    blocks = G.bvk_fc2(cr, [3.0, 0.45])
+    shells = G.shell_distances(cr, 4)
+    cl3 = G.generate_anharmonic(cr, 3, 0.5 * (shells[2] + shells[3]), 5.0, 11)
+    cl4 = G.generate_anharmonic(cr, 4, 0.5 * (shells[0] + shells[1]), 2.0, 12)
+    inp = tmp_path / "input"
+    inp.mkdir()
+    I.write_control(inp / "CONTROL", cr, (3, 3, 3), T=300.0, scalebroad=1.0, four_phonon=True)
+    G.write_fc2_phonopy(inp / "FORCE_CONSTANTS_2ND", cr, blocks)
+    G.write_fc_anharmonic(inp / "FORCE_CONSTANTS_3RD", cr, cl3)
+    G.write_fc_anharmonic(inp / "FORCE_CONSTANTS_4TH", cr, cl4)
+    s = S.load_inputs(str(inp))
+    out = tmp_path / "output"
+    res = driver.run(s, str(out), convergence=True, four_phonon=True, maxiter=50, ctx=OracleContext(s),
+                     log=lambda *a: None)
+    k_rta, k_conv, it = _by_hand(s, 300.0, it4=False)
+    assert np.allclose(res[0]["kappa_conv"], k_conv, rtol=1e-12, atol=1e-14 * np.abs(k_conv).max())
+    assert res[0]["iterations"] == it
+    assert np.isfinite(res[0]["kappa_conv"]).all() and np.trace(res[0]["kappa_conv"]) > 0
+    for name in ("BTE.Numprocess_4ph", "BTE.P3", "BTE.P4", "BTE.KappaTensorVsT_RTA", "BTE.KappaTensorVsT_CONV",
+                 os.path.join("T300K", "BTE.w_4ph"), os.path.join("T300K", "BTE.kappa_tensor")):
+        assert os.path.getsize(os.path.join(str(out), name)) > 0, name
