@@ -368,8 +368,9 @@ int fp4_eigen_dm(fp4_ctx *ctx, const fp4_globals *g, const double *lattvec, cons
  * exits.  A call needs nptk*nbands*32 + nptk*4 + nlist*4 + nlist*nbands*48
  * bytes plus 256 B of counters, each of the five parts rounded up to 256 B:
  * e.g. a 24^3 grid with 12 branches fits when List is an irreducible wedge
- * (nlist up to about 8,000 points) but not the full grid.  Larger calls
- * return FP4_E_CAPACITY before any device work; a List entry outside
+ * (nlist up to about 8,000 points) but not the full grid.  Larger calls, and
+ * calls with more than 2^31 - 2^20 work items (3*nlist*nptk), return
+ * FP4_E_CAPACITY before any device work; a List entry outside
  * [1, nptk] returns FP4_E_ARG.  The first call in each CUDA context looks up
  * the array's device address in that context, so make that call before any
  * stream capture.  All calls share the array: calls that
