@@ -122,8 +122,23 @@ def executed_flops(s, counters, npi):
     f_sigma = 27.0
     f_test = 3.0
     f_proc = 27.0 + 25.0 + 12.0 * nT + 116.0 * npi
-    f_z = s.nb * 9.0 * npi * 0 + s.nb * 9.0 * s.ifc4.ntri * 98.0  # per table build (one branch i, all j)
+    f_z = s.nb * 9.0 * s.ifc4.ntri * 98.0  # per table build (one branch i, all j)
     return nsig * f_sigma + ncand * f_test + ncontr * f_proc + nz * f_z
+
+
+def filter_stage(counters, kernel_ms, phase_a_frac, peak):
+    """Phase A alone (enumeration and the energy-conservation filter): candidates
+    tested per second and its FP64 work (27 per broadening evaluation, 3 per window
+    test) over phase A's share of the kernel time, against the FP64 peak."""
+    if not phase_a_frac or kernel_ms <= 0:
+        return None
+    t = kernel_ms / 1e3 * phase_a_frac
+    nsig, ncand = float(counters[2]), float(counters[3])
+    tf = (27.0 * nsig + 3.0 * ncand) / t / 1e12
+    return {"candidates_per_s": nsig / t, "window_tests_per_s": ncand / t, "fp64_tflops": tf,
+            "frac_of_fp64_peak": tf / peak if peak else None, "seconds": t,
+            "note": "phase A time = the event-timed kernel duration x phase A's share of the CTA cycles; "
+                    "candidates = broadening evaluations (q'', k, l kept by the channel's restrictions)"}
 
 
 def npi_of(s):
@@ -583,6 +598,7 @@ def run_ours(args):
                                   "MEASURED_PEAKS)",
                      "achieved_note": "executed FP64 flops of k4_work from its work counters / event-timed duration",
                      "ref_equivalent_tflops": last["nproc"] * ref_flops_per_process(s) / (kms / 1e3) / 1e12},
+        "filter_stage": filter_stage(cnt, kms, last["phases"].get("phase_a_frac"), peak),
         "clocks": clk, "gpu_launches": launches,
         "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
     }
